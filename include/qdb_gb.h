@@ -1,0 +1,208 @@
+/*
+ * qdb_gb.h - C ABI of the B200 GROUP BY hot path (filter -> compaction -> hash aggregate).
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an int32
+ * status whose values 0..8 are the reference's QueryEngineErrorType
+ * (qikkDB/QueryEngine/GPUError.h:17-28); values >= 100 are this library's own.
+ * Device pointers are CUDA device pointers on the current device.  `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream, which is what the
+ * reference's operators use, qikkDB/QueryEngine/GPUCore/GPUMemory.cuh:89-189).
+ *
+ * Buffers that an entry point hands back (`out` pointers) are allocated by the library
+ * on `stream` with the stream-ordered allocator and must be released with qdb_free(),
+ * mirroring GPUMemory::alloc / GPUMemory::free ownership in the reference
+ * (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:501, GPUReconstruct.cuh:296).
+ *
+ * Null masks are the reference's bit-packed `nullmask_t` (uint64_t, bit i%64 of word i/64,
+ * qikkDB/QueryEngine/GPUCore/NullValues.cuh:6-12, NullValues.cu:3-57).
+ */
+#ifndef QDB_GB_H
+#define QDB_GB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes: 0..8 mirror QueryEngineErrorType (qikkDB/QueryEngine/GPUError.h:17-28) ---- */
+enum qdb_status {
+    QDB_OK = 0,                 /* GPU_EXTENSION_SUCCESS */
+    QDB_ERROR = 1,              /* GPU_EXTENSION_ERROR (CUDA or argument error) */
+    QDB_DIVISION_BY_ZERO = 2,   /* GPU_DIVISION_BY_ZERO_ERROR */
+    QDB_INTEGER_OVERFLOW = 3,   /* GPU_INTEGER_OVERFLOW_ERROR */
+    QDB_HASH_TABLE_FULL = 4,    /* GPU_HASH_TABLE_FULL: more distinct keys than the table holds */
+    QDB_UNKNOWN_AGG_FUN = 5,    /* GPU_UNKNOWN_AGG_FUN */
+    QDB_NOT_FOUND = 6,          /* GPU_NOT_FOUND_ERROR: no CUDA device */
+    QDB_ERR_INVALID = 100,      /* bad argument (type code, size, null pointer) */
+    QDB_ERR_NOMEM = 101,        /* device allocation failed */
+    QDB_ERR_CUDA = 102,         /* a CUDA runtime call failed; see qdb_last_error() */
+    QDB_ERR_TIMEOUT = 103,      /* a bounded device-side wait gave up */
+    QDB_ERR_TOO_LARGE = 104     /* size beyond a stated maximum */
+};
+
+/* ---- element types (codes follow the reference's COLUMN_* DataType values, qikkDB/DataType.h:7-27) ---- */
+enum qdb_type {
+    QDB_INT32 = 8,   /* COLUMN_INT */
+    QDB_INT64 = 9,   /* COLUMN_LONG */
+    QDB_FLOAT = 10,  /* COLUMN_FLOAT */
+    QDB_DOUBLE = 11, /* COLUMN_DOUBLE */
+    QDB_INT8 = 15    /* COLUMN_INT8_T (filter operands / masks only) */
+};
+
+/* ---- aggregate bits (AggregationFunctions::{min,max,sum,avg,count,none},
+ *      qikkDB/QueryEngine/GPUCore/AggregationFunctions.cuh:17-366). A table may carry several
+ *      aggregates at once (one fused pass); AGG none is agg_mask == 0. ---- */
+enum qdb_agg {
+    QDB_AGG_MIN = 1,
+    QDB_AGG_MAX = 2,
+    QDB_AGG_SUM = 4,
+    QDB_AGG_AVG = 8,
+    QDB_AGG_COUNT = 16
+};
+
+/* ---- filter operators (FilterConditions::*, qikkDB/QueryEngine/GPUCore/GPUFilterConditions.cuh:9-180) ---- */
+enum qdb_cmp {
+    QDB_GREATER = 0,
+    QDB_GREATER_EQUAL = 1,
+    QDB_LESS = 2,
+    QDB_LESS_EQUAL = 3,
+    QDB_EQUAL = 4,
+    QDB_NOT_EQUAL = 5,
+    QDB_LOGICAL_AND = 6,
+    QDB_LOGICAL_OR = 7
+};
+
+/* ---- table placement hints for the aggregation pass ---- */
+enum qdb_placement {
+    QDB_PLACE_AUTO = 0,   /* choose from the capacity hint */
+    QDB_PLACE_SHARED = 1, /* per-CTA shared-memory table with global spill (low cardinality / skew) */
+    QDB_PLACE_GLOBAL = 2  /* global open-addressing table only (high cardinality) */
+};
+
+/* A predicate `col OP constant` evaluated inside the aggregation pass (the fused form of
+ * GPUBinary<OP,int8_t,T*,U>::Binary + GPUReconstruct::reconstructColKeep, which the reference
+ * runs as separate kernels, qikkDB/QueryEngine/GPUCore/GPUBinary.cuh:555-579,
+ * GPUReconstruct.cuh:272-355).  Rows whose predicate column is NULL are filtered out, as
+ * kernel_filter does (qikkDB/QueryEngine/GPUCore/GPUFilter.cuh:22-44). */
+typedef struct qdb_pred {
+    const void* col;         /* device column */
+    int32_t type;            /* qdb_type of col (INT32, INT64, FLOAT, DOUBLE) */
+    int32_t op;              /* qdb_cmp (comparison ops only) */
+    int32_t const_type;      /* qdb_type of the constant; the comparison runs in the C++ common type
+                                of (column type, constant type), as kernel_filter's `a < b` does */
+    int32_t reserved;
+    int64_t const_i;         /* the constant when const_type is INT32 or INT64 */
+    double const_f;          /* the constant when const_type is FLOAT (exactly representable) or DOUBLE */
+    const uint64_t* nulls;   /* optional null bitmask of col */
+} qdb_pred;
+
+typedef struct qdb_gb qdb_gb; /* opaque GROUP BY table */
+
+/* Last error message of the calling thread (never NULL). */
+const char* qdb_last_error(void);
+/* Library version string. */
+const char* qdb_version(void);
+/* Number of CUDA devices visible (0 when none); returns QDB_OK. */
+int32_t qdb_device_count(int32_t* out_count);
+
+/* ---- memory helpers (GPUMemory::alloc/free/copy*, qikkDB/QueryEngine/GPUCore/GPUMemory.cuh:89-189) ---- */
+int32_t qdb_malloc(void** out_ptr, int64_t bytes, void* stream);
+int32_t qdb_free(void* ptr, void* stream);
+int32_t qdb_memcpy_h2d(void* dst, const void* src, int64_t bytes, void* stream);
+int32_t qdb_memcpy_d2h(void* dst, const void* src, int64_t bytes, void* stream);
+int32_t qdb_memcpy_d2d(void* dst, const void* src, int64_t bytes, void* stream);
+int32_t qdb_memset(void* dst, int32_t byte_value, int64_t bytes, void* stream);
+int32_t qdb_stream_sync(void* stream);
+
+/* ---- GROUP BY table: GPUGroupBy<AGG,O,K,V> (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:285-790) and
+ *      the multi-key specialisation (qikkDB/QueryEngine/GPUCore/GPUGroupByMultiKey.cuh:262-1325). ----
+ *
+ * qdb_gb_create replaces the constructor GPUGroupBy(maxHashCount, keySizeMultiplier)
+ * (GPUGroupBy.cuh:313): `max_groups` = maxHashCount * keySizeMultiplier, capped at 2^30 like
+ * GB_BUFFER_SIZE_MAX (IGroupBy.h:5).  key_type is a qdb_type; n_key_cols is 1, or 2 for a composite
+ * (int32 x int32) key.  val_type is a qdb_type or 0 for a table without a value column.
+ * agg_mask is an OR of qdb_agg bits.  placement is a qdb_placement hint. */
+int32_t qdb_gb_create(qdb_gb** out, int32_t agg_mask, int32_t key_type, int32_t n_key_cols,
+                      int32_t val_type, int64_t max_groups, int32_t placement, void* stream);
+/* ~GPUGroupBy (GPUGroupBy.cuh:374-386). */
+int32_t qdb_gb_destroy(qdb_gb* gb);
+/* GetMaxHashCount (GPUGroupBy.cuh:414): the reference's keyBufferSize_ (max_groups + 1 NULL slot). */
+int32_t qdb_gb_max_hash_count(qdb_gb* gb, int64_t* out);
+/* Number of distinct non-NULL keys inserted so far (reads a device counter; synchronises stream). */
+int32_t qdb_gb_group_count(qdb_gb* gb, int64_t* out, void* stream);
+
+/* ProcessBlock (GPUGroupBy.cuh:395-410; multi-key GPUGroupByMultiKey.cuh:535-627), asynchronous:
+ * key_cols[n_key_cols] device key columns, key_nulls[n_key_cols] optional null bitmasks (array may be
+ * NULL), vals/val_nulls the value column (NULL when val_type == 0), n rows.  `pred` (optional) is a
+ * fused filter; `mask` (optional) is a precomputed int8 filter mask (non-zero = keep).  Both may be
+ * given; a row is aggregated when it passes both.  Errors raised by the kernel (HASH_TABLE_FULL) are
+ * latched in the table and returned by qdb_gb_check (the ErrorFlagSwapper::Swap step,
+ * qikkDB/QueryEngine/GPUCore/ErrorFlagSwapper.h:32-50). */
+int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
+                       const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
+                       const int8_t* mask, void* stream);
+/* Synchronises `stream`, returns and clears the latched kernel status (QDB_OK or QDB_HASH_TABLE_FULL). */
+int32_t qdb_gb_check(qdb_gb* gb, void* stream);
+/* ProcessBlock followed by the Swap check: the synchronous form the reference exposes. */
+int32_t qdb_gb_process_sync(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
+                            const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
+                            const int8_t* mask, void* stream);
+
+/* GetResults (GPUGroupBy.cuh:478-587; multi-key GPUGroupByMultiKey.cuh:742-912).
+ * For one aggregate `agg` (a single qdb_agg bit, or 0 for GROUP BY without aggregation):
+ * out_keys[n_key_cols] receive newly allocated device key columns, out_key_nulls[n_key_cols] (optional)
+ * their null bitmasks, *out_vals the values (type: V for MIN/MAX/SUM/AVG, int64 for COUNT),
+ * *out_val_nulls (optional) the value null bitmask, *out_count the group count.  An empty result yields
+ * NULL pointers and count 0 (GPUReconstruct.cuh:311-318).  Synchronises `stream` (the count is read back). */
+int32_t qdb_gb_results(qdb_gb* gb, int32_t agg, void** out_keys, uint64_t** out_key_nulls, void** out_vals,
+                       uint64_t** out_val_nulls, int64_t* out_count, void* stream);
+/* Several aggregates from one fused table in one pass: aggs[n_aggs] are qdb_agg bits, out_vals[i] and
+ * out_val_nulls[i] (optional array) receive aggregate i. */
+int32_t qdb_gb_results_multi(qdb_gb* gb, int32_t n_aggs, const int32_t* aggs, void** out_keys,
+                             uint64_t** out_key_nulls, void** out_vals, uint64_t** out_val_nulls,
+                             int64_t* out_count, void* stream);
+/* Clears the table to its freshly created state (asynchronous). */
+int32_t qdb_gb_reset(qdb_gb* gb, void* stream);
+
+/* ---- raw partial state, for merging tables across GPUs (GetResults over `tables`,
+ *      GPUGroupBy.cuh:594-790, and ReconstructRawNumbers, :433-471) ----
+ * A partial record is (key word, state words).  qdb_gb_export_partitioned writes every occupied slot,
+ * bucketed by owner = hash(key) mod n_parts, into newly allocated device buffers: *out_keys (uint64 key
+ * words, int64 for composite packing), *out_state (state words, qdb_gb_state_words() per record),
+ * *out_flags (uint8: bit0 NULL key slot, bit1 escaped key slot, bit2 composite-with-null key),
+ * and host array part_counts[n_parts]. Synchronises `stream`. */
+int32_t qdb_gb_state_words(qdb_gb* gb, int32_t* out_words);
+int32_t qdb_gb_export_partitioned(qdb_gb* gb, int32_t n_parts, uint64_t** out_keys, uint64_t** out_state,
+                                  uint8_t** out_flags, int64_t* part_counts, void* stream);
+/* Merges `n` exported records (device buffers in the export layout) into `gb` (asynchronous). */
+int32_t qdb_gb_merge_partial(qdb_gb* gb, const uint64_t* keys, const uint64_t* state, const uint8_t* flags,
+                             int64_t n, void* stream);
+
+/* ---- filter: GPUBinary<FilterConditions::OP,int8_t,L,R>::Binary
+ *      (qikkDB/QueryEngine/GPUCore/GPUBinary.cuh:555-579, kernel_filter GPUFilter.cuh:22-44) ----
+ * out_mask[i] = OP(a[i] or a, b[i] or b) && !null(i).  When a side is a constant (`*_is_col` == 0) its
+ * pointer is a HOST pointer to one value of its type.  const-const fills the mask (GPUBinary.cuh:573). */
+int32_t qdb_filter(int32_t op, int32_t a_type, int32_t a_is_col, const void* a, int32_t b_type, int32_t b_is_col,
+                   const void* b, const uint64_t* null_mask, int8_t* out_mask, int64_t n, void* stream);
+
+/* ---- compaction: GPUReconstruct (qikkDB/QueryEngine/GPUCore/GPUReconstruct.cuh:204-355, :487-640) ----
+ * qdb_reconstruct_keep: reconstructColKeep<T> with elem_bytes = sizeof(T) (1, 2, 4 or 8).  A NULL mask
+ * returns `in` itself and n (no copy), as the reference does (GPUReconstruct.cuh:320-327).
+ * null_in/out_null_mask: optional null bitmask to compact alongside. Synchronises `stream`. */
+int32_t qdb_reconstruct_keep(int32_t elem_bytes, const void* in, const int8_t* mask, int64_t n, void** out,
+                             int64_t* out_count, const uint64_t* null_in, uint64_t** out_null_mask,
+                             void* stream);
+/* GenerateIndexesKeep<int32_t,int8_t> (GPUReconstruct.cuh:518-566): int32 row indices where mask != 0. */
+int32_t qdb_generate_indexes(const int8_t* mask, int64_t n, int32_t** out, int64_t* out_count, void* stream);
+/* PrefixSum<int32_t,int8_t> (GPUReconstruct.cuh:573-583): inclusive sum of mask into out[n] (caller-owned). */
+int32_t qdb_prefix_sum(const int8_t* mask, int64_t n, int32_t* out, void* stream);
+/* CompressNullMask (GPUReconstruct.cu:756-764): uint8 array (bit0 of each byte) -> bit-packed mask
+ * (newly allocated, ceil(n/64) words). */
+int32_t qdb_compress_null_mask(const uint8_t* in, int64_t n, uint64_t** out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QDB_GB_H */

@@ -1,0 +1,289 @@
+// GROUP BY table management, result extraction and partial-state exchange: the GPUGroupBy<AGG,O,K,V>
+// operator surface (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:285-790) and its multi-key
+// specialisation (qikkDB/QueryEngine/GPUCore/GPUGroupByMultiKey.cuh:262-1325) behind the C ABI.
+#include <algorithm>
+#include <vector>
+
+#include "groupby_agg.cuh"
+
+namespace qdb {
+
+// ---------------------------------------------------------------------------------------------
+// Layout and sizing.
+// ---------------------------------------------------------------------------------------------
+static Layout make_layout(int32_t aggs, ValKind vk) {
+    Layout L;
+    const bool has_vals = vk != VK_NONE;
+    int w = 1;
+    if (has_vals || (aggs & QDB_AGG_COUNT)) L.cnt = w++;
+    if (has_vals && (aggs & (QDB_AGG_SUM | QDB_AGG_AVG))) L.sum = w++;
+    if (has_vals && (aggs & (QDB_AGG_MIN | QDB_AGG_MAX))) {
+        if (vk_is_32(vk)) {
+            L.packed = 1;
+            L.mn = L.mx = w++;
+        } else {
+            if (aggs & QDB_AGG_MIN) L.mn = w++;
+            if (aggs & QDB_AGG_MAX) L.mx = w++;
+        }
+    }
+    int W = 1;
+    while (W < w) W <<= 1;
+    L.W = W;
+    return L;
+}
+
+static uint64_t next_pow2(uint64_t x) {
+    uint64_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+__global__ void init_region_kernel(uint64_t* slots, uint64_t nslots, Layout L, int32_t vk32) {
+    const uint64_t total = nslots * static_cast<uint64_t>(L.W);
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const int w = static_cast<int>(i % L.W);
+        uint64_t v = 0;
+        if (w == 0) v = kEmpty;
+        else if (w == L.mn && L.packed) v = kPackedMinMaxInit;
+        else if (w == L.mn) v = kMinInit64;
+        else if (w == L.mx) v = kMaxInit64;
+        slots[i] = v;
+    }
+}
+
+int32_t gb_init_region(qdb_gb* gb, Region& r, cudaStream_t s) {
+    const uint64_t nslots = gb->cap + 2;
+    if (!r.slots) {
+        int32_t rc = dev_alloc(reinterpret_cast<void**>(&r.slots), nslots * gb->L.W * sizeof(uint64_t), s);
+        if (rc != QDB_OK) return rc;
+        r.mask = gb->cap - 1;
+    }
+    const DeviceInfo& di = device_info();
+    uint64_t blocks = (nslots * gb->L.W + 255) / 256;
+    if (blocks > static_cast<uint64_t>(di.sm_count) * 16) blocks = static_cast<uint64_t>(di.sm_count) * 16;
+    init_region_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(r.slots, nslots, gb->L,
+                                                                      vk_is_32(val_kind(gb->val_type)));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "init_region_kernel");
+    return QDB_OK;
+}
+
+static int32_t launch_agg(const qdb_gb* gb, const AggArgs& a, int32_t ptype, size_t smem, cudaStream_t st) {
+    const ValKind vk = val_kind(gb->val_type);
+    if (gb->n_key_cols == 2) return launch_agg_comp(a, vk, ptype, smem, st);
+    switch (gb->key_type) {
+        case QDB_INT32: return launch_agg_i32(a, vk, ptype, smem, st);
+        case QDB_INT64: return launch_agg_i64(a, vk, ptype, smem, st);
+        case QDB_FLOAT: return launch_agg_f32(a, vk, ptype, smem, st);
+        case QDB_DOUBLE: return launch_agg_f64(a, vk, ptype, smem, st);
+        default: return fail(QDB_ERR_INVALID, "unsupported key type");
+    }
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace qdb
+
+using namespace qdb;
+
+extern "C" {
+
+int32_t qdb_gb_create(qdb_gb** out, int32_t agg_mask, int32_t key_type, int32_t n_key_cols, int32_t val_type,
+                      int64_t max_groups, int32_t placement, void* stream) {
+    if (!out) return fail(QDB_ERR_INVALID, "qdb_gb_create: null out");
+    *out = nullptr;
+    if (agg_mask & ~(QDB_AGG_MIN | QDB_AGG_MAX | QDB_AGG_SUM | QDB_AGG_AVG | QDB_AGG_COUNT))
+        return fail(QDB_UNKNOWN_AGG_FUN, "qdb_gb_create: unknown aggregate bits");
+    if (n_key_cols != 1 && n_key_cols != 2) return fail(QDB_ERR_INVALID, "qdb_gb_create: n_key_cols must be 1 or 2");
+    if (n_key_cols == 2 && key_type != QDB_INT32)
+        return fail(QDB_ERR_INVALID, "qdb_gb_create: composite keys are (int32, int32)");
+    if (key_type != QDB_INT32 && key_type != QDB_INT64 && key_type != QDB_FLOAT && key_type != QDB_DOUBLE)
+        return fail(QDB_ERR_INVALID, "qdb_gb_create: unsupported key type");
+    if (val_type != 0 && val_kind(val_type) == VK_NONE)
+        return fail(QDB_ERR_INVALID, "qdb_gb_create: unsupported value type");
+    if (val_type == 0 && (agg_mask & (QDB_AGG_MIN | QDB_AGG_MAX | QDB_AGG_SUM | QDB_AGG_AVG)))
+        return fail(QDB_ERR_INVALID, "qdb_gb_create: MIN/MAX/SUM/AVG need a value column");
+    if (max_groups < 1) return fail(QDB_ERR_INVALID, "qdb_gb_create: max_groups must be >= 1");
+    if (max_groups > (int64_t(1) << 30)) max_groups = int64_t(1) << 30;  // GB_BUFFER_SIZE_MAX
+    int dev = 0;
+    QDB_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t s = as_stream(stream);
+
+    qdb_gb* gb = new qdb_gb();
+    gb->aggs = agg_mask;
+    gb->key_type = key_type;
+    gb->n_key_cols = n_key_cols;
+    gb->val_type = val_type;
+    gb->placement = placement;
+    gb->device = dev;
+    gb->capacity = max_groups;
+    gb->cap = next_pow2(std::max<uint64_t>(16, static_cast<uint64_t>(max_groups) * 3 / 2 + 1));
+    gb->L = make_layout(agg_mask, val_kind(val_type));
+    int32_t rc = dev_alloc(reinterpret_cast<void**>(&gb->counters), 2 * sizeof(unsigned long long), s);
+    if (rc == QDB_OK) rc = gb_init_region(gb, gb->main, s);
+    if (rc == QDB_OK && cudaMemsetAsync(gb->counters, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess)
+        rc = cuda_fail(cudaGetLastError(), "cudaMemsetAsync(counters)");
+    if (rc != QDB_OK) {
+        qdb_gb_destroy(gb);
+        return rc;
+    }
+    *out = gb;
+    return QDB_OK;
+}
+
+int32_t qdb_gb_destroy(qdb_gb* gb) {
+    if (!gb) return QDB_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != gb->device) cudaSetDevice(gb->device);
+    // The table may still be in use by work queued on another stream: free in stream order on the
+    // legacy stream, which orders after all blocking streams.
+    dev_free(gb->main.slots, 0);
+    dev_free(gb->aux.slots, 0);
+    dev_free(gb->counters, 0);
+    if (prev != gb->device) cudaSetDevice(prev);
+    delete gb;
+    return QDB_OK;
+}
+
+int32_t qdb_gb_max_hash_count(qdb_gb* gb, int64_t* out) {
+    if (!gb || !out) return fail(QDB_ERR_INVALID, "qdb_gb_max_hash_count: null argument");
+    *out = gb->capacity + 1;  // + 1 for the NULL key, as keyBufferSize_ (GPUGroupBy.cuh:315)
+    return QDB_OK;
+}
+
+int32_t qdb_gb_group_count(qdb_gb* gb, int64_t* out, void* stream) {
+    if (!gb || !out) return fail(QDB_ERR_INVALID, "qdb_gb_group_count: null argument");
+    unsigned long long h = 0;
+    QDB_CUDA_TRY(cudaMemcpyAsync(&h, gb->counters, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream)));
+    QDB_CUDA_TRY(cudaStreamSynchronize(as_stream(stream)));
+    *out = static_cast<int64_t>(h);
+    return QDB_OK;
+}
+
+int32_t qdb_gb_reset(qdb_gb* gb, void* stream) {
+    if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_reset: null table");
+    cudaStream_t s = as_stream(stream);
+    int32_t rc = gb_init_region(gb, gb->main, s);
+    if (rc == QDB_OK && gb->aux.slots) rc = gb_init_region(gb, gb->aux, s);
+    if (rc != QDB_OK) return rc;
+    QDB_CUDA_TRY(cudaMemsetAsync(gb->counters, 0, 2 * sizeof(unsigned long long), s));
+    return QDB_OK;
+}
+
+int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls, const void* vals,
+                       const uint64_t* val_nulls, int64_t n, const qdb_pred* pred, const int8_t* mask,
+                       void* stream) {
+    if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_process: null table");
+    if (n < 0) return fail(QDB_ERR_INVALID, "qdb_gb_process: negative row count");
+    if (n == 0) return QDB_OK;
+    if (!key_cols || !key_cols[0] || (gb->n_key_cols == 2 && !key_cols[1]))
+        return fail(QDB_ERR_INVALID, "qdb_gb_process: missing key column");
+    if (gb->val_type != 0 && !vals) return fail(QDB_ERR_INVALID, "qdb_gb_process: missing value column");
+    int32_t ptype = 0;
+    if (pred) {
+        if (!pred->col) return fail(QDB_ERR_INVALID, "qdb_gb_process: predicate without column");
+        if (pred->op < QDB_GREATER || pred->op > QDB_NOT_EQUAL)
+            return fail(QDB_ERR_INVALID, "qdb_gb_process: predicate op must be a comparison");
+        if (pred->type != QDB_INT32 && pred->type != QDB_INT64 && pred->type != QDB_FLOAT && pred->type != QDB_DOUBLE)
+            return fail(QDB_ERR_INVALID, "qdb_gb_process: unsupported predicate column type");
+        if (pred->const_type != QDB_INT32 && pred->const_type != QDB_INT64 && pred->const_type != QDB_FLOAT &&
+            pred->const_type != QDB_DOUBLE)
+            return fail(QDB_ERR_INVALID, "qdb_gb_process: unsupported predicate constant type");
+        ptype = pred->type;
+    }
+    cudaStream_t s = as_stream(stream);
+    const uint64_t* kn0 = key_nulls ? key_nulls[0] : nullptr;
+    const uint64_t* kn1 = (key_nulls && gb->n_key_cols == 2) ? key_nulls[1] : nullptr;
+    if (gb->n_key_cols == 2 && (kn0 || kn1) && !gb->aux.slots) {
+        int32_t rc = gb_init_region(gb, gb->aux, s);
+        if (rc != QDB_OK) return rc;
+    }
+
+    AggArgs a;
+    a.key0 = key_cols[0];
+    a.key1 = gb->n_key_cols == 2 ? key_cols[1] : nullptr;
+    a.knull0 = kn0;
+    a.knull1 = kn1;
+    a.vals = gb->val_type ? vals : nullptr;
+    a.vnull = gb->val_type ? val_nulls : nullptr;
+    if (pred) {
+        a.pcol = pred->col;
+        a.pnull = pred->nulls;
+        a.pc.op = pred->op;
+        a.pc.ctype = pred->const_type;
+        a.pc.ci = pred->const_i;
+        a.pc.cf = pred->const_f;
+    }
+    a.mask = mask;
+    a.n = n;
+    a.tiles = (n + kTileRows - 1) / kTileRows;
+    a.main = gb->main;
+    a.aux = gb->aux;
+    a.L = gb->L;
+    const ValKind vk = val_kind(gb->val_type);
+    a.has_sum = gb->L.sum >= 0;
+    a.has_min = (gb->aggs & QDB_AGG_MIN) && gb->L.mn >= 0;
+    a.has_max = (gb->aggs & QDB_AGG_MAX) && gb->L.mx >= 0;
+    a.counters = gb->counters;
+    a.capacity = static_cast<unsigned long long>(gb->capacity);
+    a.vec_ok = aligned16(a.key0) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
+               (!a.pcol || aligned16(a.pcol)) && (!mask || (reinterpret_cast<uintptr_t>(mask) & 3u) == 0);
+
+    // Shared-memory table sizing.
+    size_t smem = 0;
+    if (gb->placement != QDB_PLACE_GLOBAL) {
+        const DeviceInfo& di = device_info();
+        const bool has_mm = a.has_min || a.has_max;
+        const size_t bps = 8 + 4 + (a.has_sum ? 8 : 0) + (has_mm ? (vk_is_32(vk) ? 8 : 16) : 0);
+        const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024;
+        int S = 1 << 16;
+        while (S >= 256 && static_cast<size_t>(S + 2) * bps > budget) S >>= 1;
+        // A table much larger than the group count only costs initialisation and merge time.
+        const uint64_t want = next_pow2(static_cast<uint64_t>(gb->capacity) * 2 + 2);
+        if (static_cast<uint64_t>(S) > want) S = static_cast<int>(std::max<uint64_t>(want, 256));
+        if (S >= 256) {
+            const size_t S2 = S + 2;
+            a.S = S;
+            a.probe = (static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2) ? S : 16;
+            size_t off = S2 * 8;
+            if (a.has_sum) { a.so_sum = static_cast<int32_t>(off); off += S2 * 8; }
+            if (has_mm) {
+                a.so_mn = static_cast<int32_t>(off);
+                off += S2 * 8;
+                if (vk_is_32(vk)) a.so_mx = a.so_mn;
+                else { a.so_mx = static_cast<int32_t>(off); off += S2 * 8; }
+            }
+            a.so_cnt = static_cast<int32_t>(off);
+            off += S2 * 4;
+            smem = (off + 15) & ~size_t(15);
+        }
+    }
+    return launch_agg(gb, a, ptype, smem, s);
+}
+
+int32_t qdb_gb_check(qdb_gb* gb, void* stream) {
+    if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_check: null table");
+    cudaStream_t s = as_stream(stream);
+    int32_t status = 0;
+    QDB_CUDA_TRY(cudaMemcpyAsync(&status, &gb->counters[1], sizeof(status), cudaMemcpyDeviceToHost, s));
+    QDB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (status != QDB_OK) {
+        QDB_CUDA_TRY(cudaMemsetAsync(&gb->counters[1], 0, sizeof(unsigned long long), s));
+        if (status == QDB_HASH_TABLE_FULL)
+            return fail(QDB_HASH_TABLE_FULL, "GROUP BY hash table is full (more distinct keys than max_groups)");
+        return fail(status, "GROUP BY kernel reported an error");
+    }
+    return QDB_OK;
+}
+
+int32_t qdb_gb_process_sync(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
+                            const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
+                            const int8_t* mask, void* stream) {
+    int32_t rc = qdb_gb_process(gb, key_cols, key_nulls, vals, val_nulls, n, pred, mask, stream);
+    if (rc != QDB_OK) return rc;
+    return qdb_gb_check(gb, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+"""Helpers that run the reference's known-answer GROUP BY cases (tests/golden/reference_kats.json)."""
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OPS = {"greater": 0, "greaterEqual": 1, "less": 2, "lessEqual": 3, "equal": 4, "notEqual": 5}
+
+
+def load_kats():
+    with open(os.path.join(HERE, "golden", "reference_kats.json")) as f:
+        return json.load(f)["cases"]
+
+
+def kat_inputs(case):
+    """(keys list[np.int32], key_null_flags list or None, values np.int32 or None, value_null_flags or None)."""
+    if "generator" in case:
+        g = case["generator"]
+        keys = [np.arange(g["n"], dtype=np.int64) % g["modulus"]]
+        keys = [keys[0].astype(np.int32)]
+        vals = np.full(g["n"], g["value"], dtype=np.int32)
+        return keys, None, vals, None
+    keys = [np.asarray(k, dtype=np.int32) for k in case["keys"]]
+    kn = [np.asarray(x, dtype=bool) for x in case["key_nulls"]] if case.get("key_nulls") else None
+    vals = np.asarray(case["values"], dtype=np.int32) if case.get("values") is not None else None
+    vn = np.asarray(case["value_nulls"], dtype=bool) if case.get("value_nulls") else None
+    return keys, kn, vals, vn
+
+
+def expected_map(case):
+    out = {}
+    for e in case["expected"]:
+        key = tuple(None if n else k for k, n in zip(e["key"], e["key_null"]))
+        out[key] = e["value"]
+    return out
+
+
+def result_map(keys, key_nulls, values, value_nulls):
+    """Builds {key tuple (None = NULL component): value or None} from host arrays."""
+    out = {}
+    n = len(keys[0])
+    for i in range(n):
+        key = tuple(None if (key_nulls is not None and key_nulls[c] is not None and key_nulls[c][i]) else int(keys[c][i])
+                    for c in range(len(keys)))
+        if values is None:
+            v = None
+        elif value_nulls is not None and value_nulls[i]:
+            v = None
+        else:
+            v = int(values[i])
+        assert key not in out, f"duplicate group {key}"
+        out[key] = v
+    return out
