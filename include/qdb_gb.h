@@ -103,6 +103,8 @@ typedef struct qdb_gb qdb_gb; /* opaque GROUP BY table */
 const char* qdb_last_error(void);
 /* Library version string. */
 const char* qdb_version(void);
+/* Number of kernels this library has launched in the process so far (for launch accounting). */
+int64_t qdb_launch_count(void);
 /* Number of CUDA devices visible (0 when none); returns QDB_OK. */
 int32_t qdb_device_count(int32_t* out_count);
 
@@ -142,6 +144,15 @@ int32_t qdb_gb_group_count(qdb_gb* gb, int64_t* out, void* stream);
 int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
                        const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
                        const int8_t* mask, void* stream);
+/* ProcessBlock over HOST-resident columns (every pointer, including pred->col / pred->nulls and the masks, is a
+ * host pointer): the columns are uploaded in chunks of `chunk_rows` rows (rounded up to 4096; <= 0 picks 16M)
+ * through two device staging buffers, each chunk's upload overlapping the aggregation of the previous one.
+ * Host buffers should be pinned for the overlap.  Asynchronous on `stream` like qdb_gb_process; the caller keeps
+ * the host buffers alive until `stream` has passed this call.  Replaces the synchronous per-block LoadCol upload
+ * (qikkDB/GpuSqlParser/Dispatcher/GpuSqlDispatcherVMFunctions.h:185-260) in front of ProcessBlock. */
+int32_t qdb_gb_process_host(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
+                            const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
+                            const int8_t* mask, int64_t chunk_rows, void* stream);
 /* Synchronises `stream`, returns and clears the latched kernel status (QDB_OK or QDB_HASH_TABLE_FULL). */
 int32_t qdb_gb_check(qdb_gb* gb, void* stream);
 /* ProcessBlock followed by the Swap check: the synchronous form the reference exposes. */

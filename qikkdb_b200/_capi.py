@@ -61,6 +61,7 @@ PI64 = C.POINTER(C.c_int64)
 SIGNATURES = [
     ("qdb_last_error", C.c_char_p, []),
     ("qdb_version", C.c_char_p, []),
+    ("qdb_launch_count", I64, []),
     ("qdb_device_count", I32, [C.POINTER(I32)]),
     ("qdb_malloc", I32, [PP, I64, P]),
     ("qdb_free", I32, [P, P]),
@@ -74,6 +75,7 @@ SIGNATURES = [
     ("qdb_gb_max_hash_count", I32, [P, PI64]),
     ("qdb_gb_group_count", I32, [P, PI64, P]),
     ("qdb_gb_process", I32, [P, PP, PP, P, P, I64, C.POINTER(qdb_pred), P, P]),
+    ("qdb_gb_process_host", I32, [P, PP, PP, P, P, I64, C.POINTER(qdb_pred), P, I64, P]),
     ("qdb_gb_check", I32, [P, P]),
     ("qdb_gb_process_sync", I32, [P, PP, PP, P, P, I64, C.POINTER(qdb_pred), P, P]),
     ("qdb_gb_results", I32, [P, I32, PP, PP, PP, PP, PI64, P]),

@@ -26,7 +26,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
 ]
 CUDA_SOURCES = [
-    "runtime.cu", "groupby.cu", "results.cu", "exchange.cu", "filter.cu", "reconstruct.cu",
+    "runtime.cu", "groupby.cu", "results.cu", "exchange.cu", "filter.cu", "reconstruct.cu", "hostpipe.cu",
     "agg_i32.cu", "agg_i64.cu", "agg_f32.cu", "agg_f64.cu", "agg_comp.cu",
 ]
 EXTRA_CUDA_SOURCES: list[str] = []  # appended by later modules (batch, serving)

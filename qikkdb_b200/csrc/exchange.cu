@@ -121,6 +121,7 @@ int32_t qdb_gb_export_partitioned(qdb_gb* gb, int32_t n_parts, uint64_t** out_ke
     if (blocks > static_cast<uint64_t>(di.sm_count) * 8) blocks = static_cast<uint64_t>(di.sm_count) * 8;
     ex_hist_kernel<<<static_cast<unsigned>(blocks), kExThreads, n_parts * sizeof(unsigned int), s>>>(sp, n_parts,
                                                                                                         counts);
+    note_launch();
     std::vector<unsigned long long> h(n_parts);
     cudaError_t e = cudaMemcpyAsync(h.data(), counts, n_parts * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -157,6 +158,7 @@ int32_t qdb_gb_export_partitioned(qdb_gb* gb, int32_t n_parts, uint64_t** out_ke
     QDB_CUDA_TRY(cudaMemcpyAsync(cursors, offs.data(), n_parts * sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
     ex_scatter_kernel<<<static_cast<unsigned>(blocks), kExThreads, 0, s>>>(sp, n_parts, cursors, *out_keys, *out_state,
                                                                           *out_flags);
+    note_launch();
     e = cudaGetLastError();
     // The host copy source `offs` must stay alive until the copy has run.
     cudaError_t e2 = cudaStreamSynchronize(s);
@@ -184,6 +186,7 @@ int32_t qdb_gb_merge_partial(qdb_gb* gb, const uint64_t* keys, const uint64_t* s
         gb->main, gb->aux, gb->L, gb->L.sum >= 0, (gb->aggs & QDB_AGG_MIN) && gb->L.mn >= 0,
         (gb->aggs & QDB_AGG_MAX) && gb->L.mx >= 0, vk_is_32(vk), vk == VK_F32 || vk == VK_F64, keys, state, flags, n,
         gb->counters, static_cast<unsigned long long>(gb->capacity));
+    note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "merge_partial_kernel");
     return QDB_OK;

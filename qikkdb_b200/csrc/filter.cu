@@ -71,6 +71,7 @@ static int32_t launch_filter_ab(int32_t op, int a_col, const void* a, int b_col,
     else
         filter_kernel<A, B, false, true><<<grid, kFilterThreads, 0, s>>>(
             op, nullptr, host_value<A>(a), static_cast<const B*>(b), B{}, nulls, out, n, vec_ok);
+    note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "filter_kernel");
     return QDB_OK;

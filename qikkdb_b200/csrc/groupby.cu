@@ -2,6 +2,8 @@
 // operator surface (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:285-790) and its multi-key
 // specialisation (qikkDB/QueryEngine/GPUCore/GPUGroupByMultiKey.cuh:262-1325) behind the C ABI.
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "groupby_agg.cuh"
@@ -64,24 +66,149 @@ int32_t gb_init_region(qdb_gb* gb, Region& r, cudaStream_t s) {
     if (blocks > static_cast<uint64_t>(di.sm_count) * 16) blocks = static_cast<uint64_t>(di.sm_count) * 16;
     init_region_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(r.slots, nslots, gb->L,
                                                                       vk_is_32(val_kind(gb->val_type)));
+    note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "init_region_kernel");
     return QDB_OK;
 }
 
-static int32_t launch_agg(const qdb_gb* gb, const AggArgs& a, int32_t ptype, size_t smem, cudaStream_t st) {
+static int32_t launch_agg(const qdb_gb* gb, const AggArgs& a, int32_t ptype, bool nulls, size_t smem,
+                          cudaStream_t st) {
     const ValKind vk = val_kind(gb->val_type);
-    if (gb->n_key_cols == 2) return launch_agg_comp(a, vk, ptype, smem, st);
+    if (gb->n_key_cols == 2) return launch_agg_comp(a, vk, ptype, nulls, smem, st);
     switch (gb->key_type) {
-        case QDB_INT32: return launch_agg_i32(a, vk, ptype, smem, st);
-        case QDB_INT64: return launch_agg_i64(a, vk, ptype, smem, st);
-        case QDB_FLOAT: return launch_agg_f32(a, vk, ptype, smem, st);
-        case QDB_DOUBLE: return launch_agg_f64(a, vk, ptype, smem, st);
+        case QDB_INT32: return launch_agg_i32(a, vk, ptype, nulls, smem, st);
+        case QDB_INT64: return launch_agg_i64(a, vk, ptype, nulls, smem, st);
+        case QDB_FLOAT: return launch_agg_f32(a, vk, ptype, nulls, smem, st);
+        case QDB_DOUBLE: return launch_agg_f64(a, vk, ptype, nulls, smem, st);
         default: return fail(QDB_ERR_INVALID, "unsupported key type");
     }
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+static int64_t env_int(const char* name, int64_t dflt) {
+    const char* v = getenv(name);
+    return (v && *v) ? strtoll(v, nullptr, 10) : dflt;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Predicate `col OP constant` -> interval of the column type.  The comparison the reference's
+// kernel_filter makes (OP{}(a, b) on typed operands, in the C++ common type, GPUFilterConditions.cuh:9-120)
+// is monotone in the column value for <, <=, >, >=, so the set of passing values is an interval of the
+// column type (for == as well, and != is its complement).  The bounds are found by binary search over a
+// monotone ordinal of the column type, evaluating the exact typed comparison on the host; the kernel then
+// tests `(lo <= x && x <= hi) != invert`.  NaN columns values fail both bounds, so NaN passes only `!=`,
+// matching IEEE comparisons.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+struct Ordinal;
+template <>
+struct Ordinal<int32_t> {
+    static uint64_t first() { return 0; }
+    static uint64_t last() { return 0xffffffffull; }
+    static int32_t at(uint64_t o) { return static_cast<int32_t>(static_cast<uint32_t>(o) ^ 0x80000000u); }
+};
+template <>
+struct Ordinal<int64_t> {
+    static uint64_t first() { return 0; }
+    static uint64_t last() { return ~0ull; }
+    static int64_t at(uint64_t o) { return static_cast<int64_t>(o ^ 0x8000000000000000ull); }
+};
+template <>
+struct Ordinal<float> {
+    static uint64_t of(float x) { return static_cast<uint32_t>(fenc(x)) ^ 0x80000000u; }
+    static uint64_t first() { return of(-INFINITY); }
+    static uint64_t last() { return of(INFINITY); }
+    static float at(uint64_t o) { return fdec(static_cast<int32_t>(static_cast<uint32_t>(o) ^ 0x80000000u)); }
+};
+template <>
+struct Ordinal<double> {
+    static uint64_t of(double x) { return static_cast<uint64_t>(denc(x)) ^ 0x8000000000000000ull; }
+    static uint64_t first() { return of(-INFINITY); }
+    static uint64_t last() { return of(INFINITY); }
+    static double at(uint64_t o) { return ddec(static_cast<int64_t>(o ^ 0x8000000000000000ull)); }
+};
+
+template <typename T>
+static int64_t to_bits(T v) {
+    if constexpr (sizeof(T) == 4) {
+        int32_t w;
+        memcpy(&w, &v, 4);
+        return w;
+    } else {
+        int64_t w;
+        memcpy(&w, &v, 8);
+        return w;
+    }
+}
+
+template <typename T, typename C>
+static PredInterval interval_tc(int32_t op, C c) {
+    using O = Ordinal<T>;
+    const uint64_t L = O::first(), H = O::last();
+    auto p = [&](uint64_t o, int32_t opx) { return cmp_op(opx, O::at(o), c); };
+    auto last_true = [&](int32_t opx, uint64_t& out) {  // predicate non-increasing in the ordinal
+        if (!p(L, opx)) return false;
+        uint64_t lo = L, hi = H;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2 + 1;
+            if (p(mid, opx)) lo = mid;
+            else hi = mid - 1;
+        }
+        out = lo;
+        return true;
+    };
+    auto first_true = [&](int32_t opx, uint64_t& out) {  // predicate non-decreasing in the ordinal
+        if (!p(H, opx)) return false;
+        uint64_t lo = L, hi = H;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (p(mid, opx)) hi = mid;
+            else lo = mid + 1;
+        }
+        out = lo;
+        return true;
+    };
+    uint64_t a = L, b = H;
+    bool ok = false;
+    switch (op) {
+        case QDB_LESS:
+        case QDB_LESS_EQUAL: ok = last_true(op, b); break;
+        case QDB_GREATER:
+        case QDB_GREATER_EQUAL: ok = first_true(op, a); break;
+        default: ok = first_true(QDB_GREATER_EQUAL, a) && last_true(QDB_LESS_EQUAL, b) && a <= b; break;
+    }
+    PredInterval pi;
+    pi.invert = (op == QDB_NOT_EQUAL) ? 1 : 0;
+    if (ok) {
+        pi.lo = to_bits<T>(O::at(a));
+        pi.hi = to_bits<T>(O::at(b));
+    } else {  // empty: lo above hi
+        pi.lo = to_bits<T>(O::at(H));
+        pi.hi = to_bits<T>(O::at(L));
+    }
+    return pi;
+}
+
+template <typename T>
+static PredInterval interval_t(const qdb_pred& p) {
+    switch (p.const_type) {
+        case QDB_INT32: return interval_tc<T>(p.op, static_cast<int32_t>(p.const_i));
+        case QDB_INT64: return interval_tc<T>(p.op, static_cast<int64_t>(p.const_i));
+        case QDB_FLOAT: return interval_tc<T>(p.op, static_cast<float>(p.const_f));
+        default: return interval_tc<T>(p.op, p.const_f);
+    }
+}
+
+static PredInterval pred_interval(const qdb_pred& p) {
+    switch (p.type) {
+        case QDB_INT32: return interval_t<int32_t>(p);
+        case QDB_INT64: return interval_t<int64_t>(p);
+        case QDB_FLOAT: return interval_t<float>(p);
+        default: return interval_t<double>(p);
+    }
+}
 
 }  // namespace qdb
 
@@ -211,14 +338,10 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     if (pred) {
         a.pcol = pred->col;
         a.pnull = pred->nulls;
-        a.pc.op = pred->op;
-        a.pc.ctype = pred->const_type;
-        a.pc.ci = pred->const_i;
-        a.pc.cf = pred->const_f;
+        a.pi = pred_interval(*pred);
     }
     a.mask = mask;
     a.n = n;
-    a.tiles = (n + kTileRows - 1) / kTileRows;
     a.main = gb->main;
     a.aux = gb->aux;
     a.L = gb->L;
@@ -228,25 +351,70 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     a.has_max = (gb->aggs & QDB_AGG_MAX) && gb->L.mx >= 0;
     a.counters = gb->counters;
     a.capacity = static_cast<unsigned long long>(gb->capacity);
-    a.vec_ok = aligned16(a.key0) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
-               (!a.pcol || aligned16(a.pcol)) && (!mask || (reinterpret_cast<uintptr_t>(mask) & 3u) == 0);
+    const bool nulls = a.knull0 || a.knull1 || a.vnull || a.pnull;
 
-    // Shared-memory table sizing.
-    size_t smem = 0;
+    // Tile and stage plan.
+    const DeviceInfo& di = device_info();
+    const int ks = (gb->n_key_cols == 2) ? 4 : type_size(gb->key_type);
+    int Rw = static_cast<int>(env_int("QDB_AGG_ROWS_PER_WARP", 64));
+    Rw = std::max(kRowsPerWarpUnit, (Rw / kRowsPerWarpUnit) * kRowsPerWarpUnit);
+    int T = kConsumerWarps * Rw;
+    auto col_bytes = [&](int rows, int elem) { return static_cast<int32_t>(((size_t)rows * elem + 127) & ~size_t(127)); };
+    auto plan_stage = [&](int rows) {
+        StageLayout sl;
+        int32_t off = 0;
+        sl.key0 = off; off += col_bytes(rows, ks);
+        if (gb->n_key_cols == 2) { sl.key1 = off; off += col_bytes(rows, ks); }
+        if (a.vals) { sl.val = off; off += col_bytes(rows, type_size(gb->val_type)); }
+        if (a.pcol) { sl.pred = off; off += col_bytes(rows, type_size(pred->type)); }
+        if (a.mask) { sl.mask = off; off += col_bytes(rows, 1); }
+        if (a.knull0) { sl.knull0 = off; off += col_bytes(rows / 64, 8); }
+        if (a.knull1) { sl.knull1 = off; off += col_bytes(rows / 64, 8); }
+        if (a.vnull) { sl.vnull = off; off += col_bytes(rows / 64, 8); }
+        if (a.pnull) { sl.pnull = off; off += col_bytes(rows / 64, 8); }
+        sl.bytes = off;
+        return sl;
+    };
+    StageLayout sl = plan_stage(T);
+    while (Rw > kRowsPerWarpUnit && sl.bytes > 48 * 1024) {
+        Rw -= kRowsPerWarpUnit;
+        T = kConsumerWarps * Rw;
+        sl = plan_stage(T);
+    }
+    int NS = static_cast<int>(env_int("QDB_AGG_STAGES", sl.bytes * 3 <= 112 * 1024 ? 3 : 2));
+    NS = std::min(8, std::max(2, NS));
+    const bool aligned = aligned16(a.key0) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
+                         (!a.pcol || aligned16(a.pcol)) && (!mask || aligned16(mask)) &&
+                         (!a.knull0 || aligned16(a.knull0)) && (!a.knull1 || aligned16(a.knull1)) &&
+                         (!a.vnull || aligned16(a.vnull)) && (!a.pnull || aligned16(a.pnull));
+    a.T = T;
+    a.NS = NS;
+    a.sl = sl;
+    a.tiles = (n + T - 1) / T;
+    a.full_tiles = n / T;
+    a.staged = aligned && a.full_tiles > 0 && env_int("QDB_AGG_DIRECT", 0) == 0;
+    const size_t stage_area = a.staged ? static_cast<size_t>(NS) * sl.bytes : 0;
+    const size_t bar_bytes = 128;
+    const size_t list_bytes = (static_cast<size_t>(T) * 2 + 127) & ~size_t(127);
+    const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes;
+
+    // Shared-memory hash table sizing.
+    size_t hash_bytes = 0;
     if (gb->placement != QDB_PLACE_GLOBAL) {
-        const DeviceInfo& di = device_info();
         const bool has_mm = a.has_min || a.has_max;
         const size_t bps = 8 + 4 + (a.has_sum ? 8 : 0) + (has_mm ? (vk_is_32(vk) ? 8 : 16) : 0);
-        const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024;
         int S = 1 << 16;
-        while (S >= 256 && static_cast<size_t>(S + 2) * bps > budget) S >>= 1;
+        while (S >= 256 && static_cast<size_t>(S + 2) * bps + 64 > budget) S >>= 1;
         // A table much larger than the group count only costs initialisation and merge time.
         const uint64_t want = next_pow2(static_cast<uint64_t>(gb->capacity) * 2 + 2);
         if (static_cast<uint64_t>(S) > want) S = static_cast<int>(std::max<uint64_t>(want, 256));
+        const int64_t forced = env_int("QDB_AGG_SMEM_SLOTS", 0);
+        if (forced > 0 && forced < S) S = static_cast<int>(next_pow2(static_cast<uint64_t>(forced)));
         if (S >= 256) {
             const size_t S2 = S + 2;
             a.S = S;
-            a.probe = (static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2) ? S : 16;
+            a.probe = (static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2)
+                          ? S : static_cast<int>(env_int("QDB_AGG_PROBE", 16));
             size_t off = S2 * 8;
             if (a.has_sum) { a.so_sum = static_cast<int32_t>(off); off += S2 * 8; }
             if (has_mm) {
@@ -257,11 +425,16 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
             }
             a.so_cnt = static_cast<int32_t>(off);
             off += S2 * 4;
-            smem = (off + 15) & ~size_t(15);
+            hash_bytes = (off + 127) & ~size_t(127);
         }
     }
-    return launch_agg(gb, a, ptype, smem, s);
+    a.so_bar = static_cast<int32_t>(hash_bytes);
+    a.so_list = static_cast<int32_t>(hash_bytes + bar_bytes);
+    a.so_stage = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes);
+    const size_t smem = hash_bytes + bar_bytes + list_bytes + stage_area;
+    return launch_agg(gb, a, ptype, nulls, smem, s);
 }
+
 
 int32_t qdb_gb_check(qdb_gb* gb, void* stream) {
     if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_check: null table");

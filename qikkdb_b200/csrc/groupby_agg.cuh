@@ -2,33 +2,46 @@
 // reconstructColKeep -> group_by_kernel, qikkDB/QueryEngine/GPUCore/GPUFilter.cuh:22-44,
 // GPUReconstruct.cuh:29-45 and :272-355, GPUGroupBy.cuh:68-196).
 //
-// One persistent CTA per SM walks 4096-row tiles of the input columns with 128-bit evict-first
-// loads, prefetching the next tile into registers while it works on the current one.  For every row
-// it evaluates the predicate and the optional mask in registers (no mask or compacted column is
-// written to HBM), then inserts the key:
-//   * first into a per-CTA shared-memory table (bounded linear probe, shared-memory atomics), which
-//     absorbs low-cardinality and skewed (Zipf) key streams;
-//   * on a shared-memory miss, into the global open-addressing table (bounded linear probe with a
-//     64-bit atomicCAS on the key word, fire-and-forget reductions on the state words).  The first
-//     probe loads of a thread's misses are issued together so their L2 latencies overlap.
+// One persistent CTA per SM, warp-specialised:
+//   * a producer warp streams the CTA's tiles of every input column (keys, values, predicate column,
+//     mask, null words) from HBM into a ring of shared-memory stages with bulk asynchronous copies
+//     (cp.async.bulk, executed by the TMA engine) that complete on per-stage mbarriers;
+//   * 30 consumer warps take the stages in order.  For every row they evaluate the predicate as an
+//     interval test in the column's own type (the host turns `col OP constant` into [lo, hi] plus an
+//     invert flag, so the test is two compares and no branch), read the key, and insert it
+//       - first into a per-CTA shared-memory table (bounded linear probe, shared-memory atomics), which
+//         absorbs low-cardinality and skewed (Zipf) key streams,
+//       - on a miss, into the global open-addressing table (bounded linear probe, 64-bit atomicCAS on the
+//         key word, fire-and-forget reductions on the state words);
+//     then release the stage to the producer.  No mask or compacted column is written to HBM.
 // A warp that sees a low shared-memory hit rate after its first tiles stops probing shared memory.
 // At the end each CTA merges its shared-memory table into the global table.
+// Every wait on an mbarrier is bounded; a wait that gives up records QDB_ERR_TIMEOUT in the table status.
 #pragma once
 
 #include "groupby.cuh"
 
 namespace qdb {
 
-constexpr int kAggThreads = 512;
-constexpr int kItems = 8;                         // rows per thread per tile (two 4-row vectors)
-constexpr int kTileRows = kAggThreads * kItems;   // 4096
-constexpr int kDecideTile = 3;                    // tile index at which a warp judges its hit rate
+constexpr int kConsumerWarps = 30;
+constexpr int kConsumerThreads = kConsumerWarps * 32;     // 960
+constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer warp: 992 threads
+constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsumerWarps * R rows, R a multiple of 64
+constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
+constexpr uint32_t kMaxWaitIters = 1u << 24;               // bounded mbarrier waits (seconds, then give up)
 
-struct PredConst {
-    int32_t op = -1;     // qdb_cmp, -1 = no predicate
-    int32_t ctype = 0;   // qdb_type of the constant
-    int64_t ci = 0;
-    double cf = 0.0;
+// `col OP constant` as an interval of the column type: keep = (lo <= x && x <= hi) != invert.
+struct PredInterval {
+    int64_t lo = 0;     // bit pattern of the bound in the column type (floats: the IEEE bits)
+    int64_t hi = 0;
+    int32_t invert = 0;
+};
+
+// Byte offsets of the columns inside one shared-memory stage (-1 = absent).
+struct StageLayout {
+    int32_t key0 = -1, key1 = -1, val = -1, pred = -1, mask = -1;
+    int32_t knull0 = -1, knull1 = -1, vnull = -1, pnull = -1;
+    int32_t bytes = 0;  // stage size (multiple of 128)
 };
 
 struct AggArgs {
@@ -40,10 +53,15 @@ struct AggArgs {
     const uint64_t* vnull = nullptr;
     const void* pcol = nullptr;
     const uint64_t* pnull = nullptr;
-    PredConst pc;
+    PredInterval pi;
     const int8_t* mask = nullptr;
     int64_t n = 0;
-    int64_t tiles = 0;
+    int32_t T = 1920;        // rows per tile: kConsumerWarps * R with R a multiple of 64
+    int32_t NS = 3;          // stages in the ring
+    int64_t tiles = 0;       // all tiles, the last one possibly partial
+    int64_t full_tiles = 0;  // tiles with T rows
+    int32_t staged = 0;      // 1: full tiles arrive by bulk copy; 0: every tile is read directly from HBM
+    StageLayout sl;
     Region main;
     Region aux;
     Layout L;
@@ -52,19 +70,15 @@ struct AggArgs {
     int32_t has_max = 0;
     unsigned long long* counters = nullptr;  // [0] groups, [1] status
     unsigned long long capacity = 0;
-    int32_t S = 0;       // shared-memory slots (power of two) or 0 for a global-only pass
+    int32_t S = 0;       // shared-memory hash slots (power of two) or 0 for a global-only pass
     int32_t probe = 0;   // shared-memory probe limit
-    int32_t vec_ok = 0;  // all column pointers 16-byte aligned
-    // byte offsets of the shared-memory arrays (S + 2 entries each)
-    int32_t so_sum = 0, so_mn = 0, so_mx = 0, so_cnt = 0;
+    // byte offsets inside dynamic shared memory
+    int32_t so_stage = 0, so_bar = 0, so_list = 0;
+    int32_t so_sum = 0, so_mn = 0, so_mx = 0, so_cnt = 0;  // hash arrays (keys at offset 0), S + 2 entries each
 };
 
-// ---------------------------------------------------------------------------------------------
-// Predicate: `col OP constant` in the C++ common type of (column type, constant type), exactly as
-// kernel_filter evaluates OP{}(a, b) on typed operands (GPUFilterConditions.cuh:9-120).
-// ---------------------------------------------------------------------------------------------
 template <typename A, typename B>
-__device__ __forceinline__ bool cmp_op(int32_t op, A a, B b) {
+__host__ __device__ __forceinline__ bool cmp_op(int32_t op, A a, B b) {
     switch (op) {
         case QDB_GREATER: return a > b;
         case QDB_GREATER_EQUAL: return a >= b;
@@ -78,24 +92,22 @@ __device__ __forceinline__ bool cmp_op(int32_t op, A a, B b) {
     }
 }
 
-template <typename PT>
-__device__ __forceinline__ bool eval_pred(const PredConst& pc, PT a) {
-    switch (pc.ctype) {
-        case QDB_INT32: return cmp_op(pc.op, a, static_cast<int32_t>(pc.ci));
-        case QDB_INT64: return cmp_op(pc.op, a, static_cast<int64_t>(pc.ci));
-        case QDB_FLOAT: return cmp_op(pc.op, a, static_cast<float>(pc.cf));
-        case QDB_DOUBLE: return cmp_op(pc.op, a, pc.cf);
-        case QDB_INT8: return cmp_op(pc.op, a, static_cast<int8_t>(pc.ci));
-        default: return false;
-    }
-}
-
 struct NoPred {};
 
-// ---------------------------------------------------------------------------------------------
-// 4-row vector loads.  Row r0 is a multiple of 4; `full` means rows r0..r0+3 are all < n and the
-// pointer is 16-byte aligned.
-// ---------------------------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ __forceinline__ T from_bits(int64_t b) {
+    T v;
+    if constexpr (sizeof(T) == 4) {
+        const int32_t w = static_cast<int32_t>(b);
+        memcpy(&v, &w, 4);
+    } else {
+        memcpy(&v, &b, 8);
+    }
+    return v;
+}
+
+// 4-row vector loads (used by the standalone filter kernel).  Row r0 is a multiple of 4; `full` means
+// rows r0..r0+3 are all < n and the pointer is 16-byte aligned.
 template <typename T>
 __device__ __forceinline__ void load4(const T* __restrict__ p, int64_t r0, int64_t n, bool full, T (&out)[4]) {
     if (full) {
@@ -120,6 +132,55 @@ __device__ __forceinline__ void load4(const T* __restrict__ p, int64_t r0, int64
 #pragma unroll
         for (int e = 0; e < 4; ++e) out[e] = (r0 + e < n) ? p[r0 + e] : T{};
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// mbarrier and bulk-copy primitives (PTX ISA: mbarrier, cp.async.bulk).
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `parity` of `bar`; gives up after kMaxWaitIters tries and records QDB_ERR_TIMEOUT.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long* counters) {
+    for (uint32_t it = 0; it < kMaxWaitIters; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it >= 16) __nanosleep(128);
+    }
+    atomicExch(reinterpret_cast<int*>(&counters[1]), static_cast<int>(QDB_ERR_TIMEOUT));
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -237,10 +298,17 @@ __device__ __forceinline__ void g_merge(uint64_t* slot, const Layout& L, bool ha
     }
 }
 
+// Slot index hash of the shared-memory table: Fibonacci hashing of the folded 64-bit key word
+// (multiplicative hashing, Knuth TAOCP vol. 3, 6.4), keeping the top log2(S) bits.
+__device__ __forceinline__ uint32_t smem_hash(uint64_t kw, int shift) {
+    const uint32_t f = static_cast<uint32_t>(kw) ^ static_cast<uint32_t>(kw >> 32);
+    return (f * 0x9e3779b1u) >> shift;
+}
+
 // Shared-memory probe.  Returns the slot, or -1 after `P` probes.  *found is set when the key was
 // already present (a reuse rather than a first claim).
-__device__ __forceinline__ int s_find(uint64_t* skey, int S, int P, uint64_t key, uint64_t h, bool* found) {
-    uint32_t s = static_cast<uint32_t>(h >> 40) & static_cast<uint32_t>(S - 1);
+__device__ __forceinline__ int s_find(uint64_t* skey, int S, int P, uint64_t key, uint32_t h, bool* found) {
+    uint32_t s = h & static_cast<uint32_t>(S - 1);
     for (int p = 0; p < P; ++p) {
         const uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&skey[s]);
         if (cur == key) {
@@ -285,194 +353,224 @@ __device__ __forceinline__ void s_acc_row(unsigned char* sm, const AggArgs& a, i
 
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type
-// (int32_t when the table has no value column); PT: predicate column type or NoPred.
+// (int32_t when the table has no value column); PT: predicate column type or NoPred; NULLS: some null
+// mask (key, value or predicate) is present.
 // ---------------------------------------------------------------------------------------------
-template <typename KT, bool COMP, typename VT, typename PT>
+template <typename KT, bool COMP, typename VT, typename PT, bool NULLS>
 __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a) {
-    extern __shared__ __align__(16) unsigned char sm[];
+    extern __shared__ __align__(128) unsigned char sm[];
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
-    using PL = typename std::conditional<HAS_PRED, PT, int8_t>::type;  // storage type for predicate lanes
+    using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
 
     const int S = a.S;
     const int S2 = S ? S + 2 : 0;
     uint64_t* skey = reinterpret_cast<uint64_t*>(sm);
+    uint64_t* full_bar = reinterpret_cast<uint64_t*>(sm + a.so_bar);
+    uint64_t* empty_bar = full_bar + a.NS;
     const bool has_mm = a.has_min || a.has_max;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
 
-    if (S) {
-        for (int i = threadIdx.x; i < S2; i += blockDim.x) {
-            skey[i] = kEmpty;
-            reinterpret_cast<unsigned int*>(sm + a.so_cnt)[i] = 0u;
-            if (a.has_sum) reinterpret_cast<unsigned long long*>(sm + a.so_sum)[i] = 0ull;
-            if (has_mm) {
-                if (sizeof(VT) == 4) {
-                    reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kPackedMinMaxInit;
-                } else {
-                    reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kMinInit64;
-                    reinterpret_cast<unsigned long long*>(sm + a.so_mx)[i] = kMaxInit64;
-                }
+    for (int i = threadIdx.x; i < S2; i += blockDim.x) {
+        skey[i] = kEmpty;
+        reinterpret_cast<unsigned int*>(sm + a.so_cnt)[i] = 0u;
+        if (a.has_sum) reinterpret_cast<unsigned long long*>(sm + a.so_sum)[i] = 0ull;
+        if (has_mm) {
+            if (sizeof(VT) == 4) {
+                reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kPackedMinMaxInit;
+            } else {
+                reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kMinInit64;
+                reinterpret_cast<unsigned long long*>(sm + a.so_mx)[i] = kMaxInit64;
             }
         }
     }
+    if (threadIdx.x == 0 && a.staged) {
+        for (int s = 0; s < a.NS; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], kConsumerWarps);
+        }
+        mbar_fence_init();
+    }
     __syncthreads();
 
-    const bool has_vals = a.vals != nullptr;
-    const KT* __restrict__ k0p = static_cast<const KT*>(a.key0);
-    const KT* __restrict__ k1p = static_cast<const KT*>(a.key1);
-    const VT* __restrict__ vp = static_cast<const VT*>(a.vals);
-    const PL* __restrict__ pp = static_cast<const PL*>(a.pcol);
+    const int64_t my_tiles =
+        (a.tiles > static_cast<int64_t>(blockIdx.x)) ? (a.tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
     const int W = a.L.W;
+    const int T = a.T;
 
-    bool use_smem = S > 0;
-    unsigned my_hits = 0, my_tries = 0;
-
-    // Register fragments of the current and the next tile.
-    KT ck0[2][4], ck1[2][4], nk0[2][4], nk1[2][4];
-    VT cv[2][4], nv[2][4];
-    PL cp[2][4], np[2][4];
-    uint32_t cm[2], nm[2];  // 4 mask bytes per vector
-
-    auto row0 = [&](int64_t tile, int j) -> int64_t {
-        return tile * kTileRows + (static_cast<int64_t>(j) * kAggThreads + threadIdx.x) * 4;
-    };
-    auto load_tile = [&](int64_t tile, KT (&k0)[2][4], KT (&k1)[2][4], VT (&v)[2][4], PL (&p)[2][4],
-                         uint32_t (&m)[2]) {
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int64_t r0 = row0(tile, j);
-            const bool full = a.vec_ok && (r0 + 4 <= a.n);
-            if (r0 >= a.n) continue;
-            load4<KT>(k0p, r0, a.n, full, k0[j]);
-            if constexpr (COMP) load4<KT>(k1p, r0, a.n, full, k1[j]);
-            if (has_vals) load4<VT>(vp, r0, a.n, full, v[j]);
-            if constexpr (HAS_PRED) load4<PL>(pp, r0, a.n, full, p[j]);
-            if (a.mask) {
-                int8_t mb[4];
-                load4<int8_t>(a.mask, r0, a.n, full, mb);
-                memcpy(&m[j], mb, 4);
+    if (warp == kConsumerWarps) {
+        // ---------------- producer warp: one elected lane issues the bulk copies ----------------
+        if (lane == 0 && a.staged) {
+            const StageLayout& sl = a.sl;
+            int64_t q = 0;
+            for (; q < my_tiles; ++q) {
+                const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
+                if (tile >= a.full_tiles) break;  // the partial last tile is read directly
+                const int s = static_cast<int>(q % a.NS);
+                if (q >= a.NS && !mbar_wait(&empty_bar[s], static_cast<uint32_t>((q / a.NS - 1) & 1), a.counters))
+                    break;
+                unsigned char* st = sm + a.so_stage + static_cast<size_t>(s) * sl.bytes;
+                const int64_t r0 = tile * T;
+                const uint32_t words = static_cast<uint32_t>(T / 64) * 8u;
+                uint32_t tx = static_cast<uint32_t>(T) * sizeof(KT) * (COMP ? 2 : 1);
+                if (sl.val >= 0) tx += static_cast<uint32_t>(T) * sizeof(VT);
+                if (sl.pred >= 0) tx += static_cast<uint32_t>(T) * sizeof(PL);
+                if (sl.mask >= 0) tx += static_cast<uint32_t>(T);
+                tx += words * ((sl.knull0 >= 0) + (sl.knull1 >= 0) + (sl.vnull >= 0) + (sl.pnull >= 0));
+                fence_proxy_async_smem();
+                mbar_arrive_expect_tx(&full_bar[s], tx);
+                bulk_g2s(st + sl.key0, static_cast<const KT*>(a.key0) + r0, T * sizeof(KT), &full_bar[s]);
+                if (COMP) bulk_g2s(st + sl.key1, static_cast<const KT*>(a.key1) + r0, T * sizeof(KT), &full_bar[s]);
+                if (sl.val >= 0) bulk_g2s(st + sl.val, static_cast<const VT*>(a.vals) + r0, T * sizeof(VT), &full_bar[s]);
+                if (sl.pred >= 0) bulk_g2s(st + sl.pred, static_cast<const PL*>(a.pcol) + r0, T * sizeof(PL), &full_bar[s]);
+                if (sl.mask >= 0) bulk_g2s(st + sl.mask, a.mask + r0, T, &full_bar[s]);
+                if (sl.knull0 >= 0) bulk_g2s(st + sl.knull0, a.knull0 + r0 / 64, words, &full_bar[s]);
+                if (sl.knull1 >= 0) bulk_g2s(st + sl.knull1, a.knull1 + r0 / 64, words, &full_bar[s]);
+                if (sl.vnull >= 0) bulk_g2s(st + sl.vnull, a.vnull + r0 / 64, words, &full_bar[s]);
+                if (sl.pnull >= 0) bulk_g2s(st + sl.pnull, a.pnull + r0 / 64, words, &full_bar[s]);
+            }
+            // Drain: every issued stage must have been consumed (so no copy is still in flight) before exit.
+            for (int64_t d = (q > a.NS ? q - a.NS : 0); d < q; ++d) {
+                const int s = static_cast<int>(d % a.NS);
+                if (!mbar_wait(&empty_bar[s], static_cast<uint32_t>((d / a.NS) & 1), a.counters)) break;
             }
         }
-    };
-
-    int64_t tile = blockIdx.x;
-    if (tile < a.tiles) load_tile(tile, ck0, ck1, cv, cp, cm);
-
-    for (int it = 0; tile < a.tiles; ++it, tile += gridDim.x) {
-        const int64_t next = tile + gridDim.x;
-        if (next < a.tiles) load_tile(next, nk0, nk1, nv, np, nm);
-
-        // Pass 1: predicate, key word and the shared-memory table.
-        uint64_t kw[8];
-        uint32_t kinds = 0;  // 2 bits per item
-        uint32_t pend = 0;   // items still to insert into the global table
-        uint32_t cntit = 0;  // items whose value is aggregated (non-NULL value, or no value column)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int64_t r0 = row0(tile, j);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int i = j * 4 + e;
-                const int64_t r = r0 + e;
-                kw[i] = 0;
-                int kind = KK_NORMAL;
-                if (r >= a.n) continue;
-                bool keep = true;
-                if constexpr (HAS_PRED) keep = eval_pred<PT>(a.pc, cp[j][e]) && !null_bit(a.pnull, r);
-                if (a.mask) keep = keep && (((cm[j] >> (8 * e)) & 0xffu) != 0u);
-                if (!keep) continue;
-                if constexpr (COMP) {
-                    const bool n0 = null_bit(a.knull0, r);
-                    const bool n1 = null_bit(a.knull1, r);
-                    if (n0 || n1) {
-                        kind = KK_AUX;
-                        const uint32_t other = n0 ? (n1 ? 0u : static_cast<uint32_t>(ck1[j][e]))
-                                                  : static_cast<uint32_t>(ck0[j][e]);
-                        kw[i] = (static_cast<uint64_t>((n0 ? 1u : 0u) | (n1 ? 2u : 0u)) << 32) | other;
-                    } else {
-                        kw[i] = composite_word(static_cast<int32_t>(ck0[j][e]), static_cast<int32_t>(ck1[j][e]));
-                        kind = (kw[i] == kEmpty) ? KK_ESCAPE : KK_NORMAL;
-                    }
-                } else {
-                    if (null_bit(a.knull0, r)) {
-                        kind = KK_NULL;
-                    } else {
-                        kw[i] = key_word(ck0[j][e]);
-                        kind = (kw[i] == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+    } else {
+        // ---------------- consumer warps ----------------
+        // Warp w owns rows [w*R, (w+1)*R) of every tile (R = T / kConsumerWarps).  Phase A evaluates the
+        // predicate and mask for all of them and compacts the passing row indices into a per-warp list;
+        // phase B inserts the passing rows with every lane busy.
+        const bool has_vals = a.vals != nullptr;
+        const PL plo = HAS_PRED ? from_bits<PL>(a.pi.lo) : PL{};
+        const PL phi = HAS_PRED ? from_bits<PL>(a.pi.hi) : PL{};
+        const bool pinv = a.pi.invert != 0;
+        bool use_smem = S > 0;
+        unsigned my_hits = 0, my_tries = 0;
+        const int R = T / kConsumerWarps;
+        uint16_t* list = reinterpret_cast<uint16_t*>(sm + a.so_list) + warp * R;
+        const uint32_t lt_mask = (1u << lane) - 1u;
+        const int smem_shift = 32 - (31 - __clz(S > 0 ? S : 1));
+        for (int64_t q = 0; q < my_tiles; ++q) {
+            const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
+            const bool staged = a.staged && tile < a.full_tiles;
+            const int s = static_cast<int>(q % a.NS);
+            if (staged && !mbar_wait(&full_bar[s], static_cast<uint32_t>((q / a.NS) & 1), a.counters)) break;
+            const unsigned char* st = sm + a.so_stage + static_cast<size_t>(s) * a.sl.bytes;
+            const int64_t base = tile * T;
+            const bool skip = ((q & 15) == 0) && __any_sync(0xffffffffu, table_full(a.counters));
+            // Phase A: filter and compact.
+            int count = 0;
+            for (int j = 0; j < R && !skip; j += 32) {
+                const int i = warp * R + j + lane;
+                const int64_t r = base + i;
+                bool keep = r < a.n;
+                if (keep) {
+                    if (a.mask) keep = (staged ? reinterpret_cast<const int8_t*>(st + a.sl.mask)[i] : a.mask[r]) != 0;
+                    if constexpr (HAS_PRED) {
+                        const PL pv = staged ? reinterpret_cast<const PL*>(st + a.sl.pred)[i]
+                                             : static_cast<const PL*>(a.pcol)[r];
+                        keep = keep && (((pv >= plo) && (pv <= phi)) != pinv);
+                        if constexpr (NULLS) {
+                            if (a.pnull) {
+                                const bool pn = staged ? ((reinterpret_cast<const uint64_t*>(st + a.sl.pnull)[i >> 6] >> (i & 63)) & 1)
+                                                       : null_bit(a.pnull, r);
+                                keep = keep && !pn;
+                            }
+                        }
                     }
                 }
-                kinds |= static_cast<uint32_t>(kind) << (2 * i);
-                const bool agg_it = !has_vals || !null_bit(a.vnull, r);
-                if (agg_it) cntit |= 1u << i;
-                int s = -1;
+                const uint32_t b = __ballot_sync(0xffffffffu, keep);
+                if (keep) list[count + __popc(b & lt_mask)] = static_cast<uint16_t>(i);
+                count += __popc(b);
+            }
+            __syncwarp();
+            // Phase B: insert the passing rows.
+            for (int e = lane; e < count; e += 32) {
+                const int i = list[e];
+                const int64_t r = base + i;
+                KT k0, k1 = KT{};
+                VT v = VT{};
+                bool kn0 = false, kn1 = false, vn = false;
+                if (staged) {
+                    k0 = reinterpret_cast<const KT*>(st + a.sl.key0)[i];
+                    if constexpr (COMP) k1 = reinterpret_cast<const KT*>(st + a.sl.key1)[i];
+                    if (has_vals) v = reinterpret_cast<const VT*>(st + a.sl.val)[i];
+                    if constexpr (NULLS) {
+                        const int wi = i >> 6, bb = i & 63;
+                        if (a.sl.knull0 >= 0) kn0 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull0)[wi] >> bb) & 1;
+                        if (a.sl.knull1 >= 0) kn1 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull1)[wi] >> bb) & 1;
+                        if (a.sl.vnull >= 0) vn = (reinterpret_cast<const uint64_t*>(st + a.sl.vnull)[wi] >> bb) & 1;
+                    }
+                } else {
+                    k0 = static_cast<const KT*>(a.key0)[r];
+                    if constexpr (COMP) k1 = static_cast<const KT*>(a.key1)[r];
+                    if (has_vals) v = static_cast<const VT*>(a.vals)[r];
+                    if constexpr (NULLS) {
+                        kn0 = null_bit(a.knull0, r);
+                        kn1 = null_bit(a.knull1, r);
+                        vn = null_bit(a.vnull, r);
+                    }
+                }
+                uint64_t kw;
+                int kind;
+                if constexpr (COMP) {
+                    if (kn0 || kn1) {
+                        kind = KK_AUX;
+                        const uint32_t other = kn0 ? (kn1 ? 0u : static_cast<uint32_t>(k1)) : static_cast<uint32_t>(k0);
+                        kw = (static_cast<uint64_t>((kn0 ? 1u : 0u) | (kn1 ? 2u : 0u)) << 32) | other;
+                    } else {
+                        kw = composite_word(static_cast<int32_t>(k0), static_cast<int32_t>(k1));
+                        kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                    }
+                } else {
+                    if (kn0) {
+                        kind = KK_NULL;
+                        kw = 0;
+                    } else {
+                        kw = key_word(k0);
+                        kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                    }
+                }
+                const bool agg_it = !has_vals || !vn;
+                int slot_s = -1;
                 if (use_smem && kind != KK_AUX) {
                     if (kind == KK_NORMAL) {
                         bool found = false;
-                        s = s_find(skey, S, a.probe, kw[i], mix64(kw[i]), &found);
+                        slot_s = s_find(skey, S, a.probe, kw, smem_hash(kw, smem_shift), &found);
                         ++my_tries;
                         my_hits += found ? 1u : 0u;
                     } else {
-                        s = S + (kind == KK_ESCAPE ? 1 : 0);
-                        if (*reinterpret_cast<volatile uint64_t*>(&skey[s]) == kEmpty)
-                            atomicCAS(reinterpret_cast<unsigned long long*>(&skey[s]), kEmpty, 0ull);
+                        slot_s = S + (kind == KK_ESCAPE ? 1 : 0);
+                        if (*reinterpret_cast<volatile uint64_t*>(&skey[slot_s]) == kEmpty)
+                            atomicCAS(reinterpret_cast<unsigned long long*>(&skey[slot_s]), kEmpty, 0ull);
                     }
                 }
-                if (s >= 0) {
-                    if (agg_it) s_acc_row<VT>(sm, a, s, has_vals ? cv[j][e] : VT{}, has_vals);
-                } else {
-                    pend |= 1u << i;
+                if (slot_s >= 0) {
+                    if (agg_it) s_acc_row<VT>(sm, a, slot_s, v, has_vals);
+                    continue;
                 }
-            }
-        }
-
-        // Pass 2: global table for the shared-memory misses; first probes issued together.
-        if (pend) {
-            uint64_t first[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                first[i] = 0;
-                const int kind = (kinds >> (2 * i)) & 3;
-                if (((pend >> i) & 1u) && (kind == KK_NORMAL || kind == KK_AUX)) {
-                    const Region& R = (kind == KK_AUX) ? a.aux : a.main;
-                    first[i] = ld_volatile_u64(R.slots + (mix64(kw[i]) & R.mask) * W);
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                if (!((pend >> i) & 1u)) continue;
-                const int kind = (kinds >> (2 * i)) & 3;
                 uint64_t* slot;
                 if (kind == KK_NORMAL || kind == KK_AUX) {
-                    const Region& R = (kind == KK_AUX) ? a.aux : a.main;
-                    slot = g_find_from(R, W, kw[i], mix64(kw[i]) & R.mask, first[i], a.counters, a.capacity);
+                    const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
+                    slot = g_find(Rg, W, kw, mix64(kw), a.counters, a.capacity);
                 } else {
                     slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, a.counters, a.capacity);
                 }
-                if (slot && ((cntit >> i) & 1u)) {
-                    if (has_vals) g_acc_row<VT>(slot, a, cv[i >> 2][i & 3]);
+                if (slot && agg_it) {
+                    if (has_vals) g_acc_row<VT>(slot, a, v);
                     else g_count_row(slot, a.L);
                 }
             }
-        }
-
-        // Warp-uniform control: stop on a full table; judge the shared-memory hit rate once.
-        if (__any_sync(0xffffffffu, table_full(a.counters))) break;
-        if (it == kDecideTile && use_smem) {
-            const unsigned hits = __reduce_add_sync(0xffffffffu, my_hits);
-            const unsigned tries = __reduce_add_sync(0xffffffffu, my_tries);
-            if (tries >= 256 && hits * 8u < tries) use_smem = false;
-        }
-
-        if (next < a.tiles) {
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    ck0[j][e] = nk0[j][e];
-                    if constexpr (COMP) ck1[j][e] = nk1[j][e];
-                    cv[j][e] = nv[j][e];
-                    cp[j][e] = np[j][e];
-                }
-#pragma unroll
-            for (int j = 0; j < 2; ++j) cm[j] = nm[j];
+            if (staged) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty_bar[s]);
+            }
+            if (q == kDecideTile && use_smem) {
+                const unsigned hits = __reduce_add_sync(0xffffffffu, my_hits);
+                const unsigned tries = __reduce_add_sync(0xffffffffu, my_tries);
+                if (tries >= 256 && hits * 8u < tries) use_smem = false;
+            }
+            __syncwarp();
         }
     }
 
@@ -505,10 +603,10 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
     }
 }
 
-// Launches the kernel for one (key, value, predicate) type combination.
-template <typename KT, bool COMP, typename VT, typename PT>
+// Launches the kernel for one type combination: one persistent CTA per SM.
+template <typename KT, bool COMP, typename VT, typename PT, bool NULLS>
 int32_t launch_agg_t(const AggArgs& a, size_t smem, cudaStream_t st) {
-    auto kern = gb_agg_kernel<KT, COMP, VT, PT>;
+    auto kern = gb_agg_kernel<KT, COMP, VT, PT, NULLS>;
     const DeviceInfo& di = device_info();
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -522,40 +620,46 @@ int32_t launch_agg_t(const AggArgs& a, size_t smem, cudaStream_t st) {
     if (grid > a.tiles) grid = a.tiles;
     if (grid < 1) return QDB_OK;
     kern<<<static_cast<unsigned>(grid), kAggThreads, smem, st>>>(a);
+    note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "gb_agg_kernel launch");
     return QDB_OK;
 }
 
+template <typename KT, bool COMP, typename VT, typename PT>
+int32_t launch_agg_n(const AggArgs& a, bool nulls, size_t smem, cudaStream_t st) {
+    return nulls ? launch_agg_t<KT, COMP, VT, PT, true>(a, smem, st) : launch_agg_t<KT, COMP, VT, PT, false>(a, smem, st);
+}
+
 template <typename KT, bool COMP, typename VT>
-int32_t launch_agg_p(const AggArgs& a, int32_t ptype, size_t smem, cudaStream_t st) {
+int32_t launch_agg_p(const AggArgs& a, int32_t ptype, bool nulls, size_t smem, cudaStream_t st) {
     switch (ptype) {
-        case 0: return launch_agg_t<KT, COMP, VT, NoPred>(a, smem, st);
-        case QDB_INT32: return launch_agg_t<KT, COMP, VT, int32_t>(a, smem, st);
-        case QDB_INT64: return launch_agg_t<KT, COMP, VT, int64_t>(a, smem, st);
-        case QDB_FLOAT: return launch_agg_t<KT, COMP, VT, float>(a, smem, st);
-        case QDB_DOUBLE: return launch_agg_t<KT, COMP, VT, double>(a, smem, st);
+        case 0: return launch_agg_n<KT, COMP, VT, NoPred>(a, nulls, smem, st);
+        case QDB_INT32: return launch_agg_n<KT, COMP, VT, int32_t>(a, nulls, smem, st);
+        case QDB_INT64: return launch_agg_n<KT, COMP, VT, int64_t>(a, nulls, smem, st);
+        case QDB_FLOAT: return launch_agg_n<KT, COMP, VT, float>(a, nulls, smem, st);
+        case QDB_DOUBLE: return launch_agg_n<KT, COMP, VT, double>(a, nulls, smem, st);
         default: return fail(QDB_ERR_INVALID, "unsupported predicate column type");
     }
 }
 
 template <typename KT, bool COMP>
-int32_t launch_agg_k(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st) {
+int32_t launch_agg_k(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st) {
     switch (vk) {
         case VK_NONE:
-        case VK_I32: return launch_agg_p<KT, COMP, int32_t>(a, ptype, smem, st);
-        case VK_I64: return launch_agg_p<KT, COMP, int64_t>(a, ptype, smem, st);
-        case VK_F32: return launch_agg_p<KT, COMP, float>(a, ptype, smem, st);
-        case VK_F64: return launch_agg_p<KT, COMP, double>(a, ptype, smem, st);
+        case VK_I32: return launch_agg_p<KT, COMP, int32_t>(a, ptype, nulls, smem, st);
+        case VK_I64: return launch_agg_p<KT, COMP, int64_t>(a, ptype, nulls, smem, st);
+        case VK_F32: return launch_agg_p<KT, COMP, float>(a, ptype, nulls, smem, st);
+        case VK_F64: return launch_agg_p<KT, COMP, double>(a, ptype, nulls, smem, st);
         default: return fail(QDB_ERR_INVALID, "unsupported value type");
     }
 }
 
 // Per-key-type entry points, each instantiated in its own translation unit.
-int32_t launch_agg_i32(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
-int32_t launch_agg_i64(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
-int32_t launch_agg_f32(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
-int32_t launch_agg_f64(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
-int32_t launch_agg_comp(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
+int32_t launch_agg_i32(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
+int32_t launch_agg_i64(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
+int32_t launch_agg_f32(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
+int32_t launch_agg_f64(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
+int32_t launch_agg_comp(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
 
 }  // namespace qdb

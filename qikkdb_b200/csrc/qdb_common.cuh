@@ -35,6 +35,9 @@ struct DeviceInfo {
 };
 const DeviceInfo& device_info();
 
+// Counts this library's kernel launches (reported by qdb_launch_count()).
+void note_launch(int64_t n = 1);
+
 // Stream-ordered allocation helpers (the pool keeps freed blocks for reuse).
 int32_t dev_alloc(void** p, size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);

@@ -184,7 +184,9 @@ static int32_t count_and_scan(const int8_t* mask, int64_t n, bool sum_values, lo
     const int vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0;
     if (sum_values) rc_sum_kernel<<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(mask, n, *offsets);
     else rc_count_kernel<<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(mask, n, vec, *offsets);
+    note_launch();
     rc_scan_kernel<<<1, kRcThreads, 0, s>>>(*offsets, ntiles);
+    note_launch();
     if (total) {
         cudaError_t e = cudaMemcpyAsync(total, *offsets + ntiles, sizeof(long long), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -207,6 +209,7 @@ static void launch_scatter(const void* in, const int8_t* mask, int64_t n, const 
     const int vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0;
     rc_scatter_kernel<T><<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(
         static_cast<const T*>(in), mask, n, vec, offs, static_cast<T*>(out), null_in, null_out);
+    note_launch();
 }
 
 }  // namespace qdb
@@ -287,6 +290,7 @@ int32_t qdb_generate_indexes(const int8_t* mask, int64_t n, int32_t** out, int64
             const int64_t ntiles = (n + kRcTile - 1) / kRcTile;
             const int vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0;
             rc_indexes_kernel<<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(mask, n, vec, offs, *out);
+            note_launch();
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) rc = cuda_fail(e, "rc_indexes_kernel");
         }
@@ -305,6 +309,7 @@ int32_t qdb_prefix_sum(const int8_t* mask, int64_t n, int32_t* out, void* stream
     if (rc != QDB_OK) return rc;
     const int64_t ntiles = (n + kRcTile - 1) / kRcTile;
     rc_prefix_kernel<<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(mask, n, offs, out);
+    note_launch();
     cudaError_t e = cudaGetLastError();
     dev_free(offs, s);
     if (e != cudaSuccess) return cuda_fail(e, "rc_prefix_kernel");
@@ -325,6 +330,7 @@ int32_t qdb_compress_null_mask(const uint8_t* in, int64_t n, uint64_t** out, voi
     int64_t blocks = ((n + 31) / 32 * 32 + 255) / 256;
     if (blocks > static_cast<int64_t>(di.sm_count) * 16) blocks = static_cast<int64_t>(di.sm_count) * 16;
     rc_compress_kernel<<<static_cast<unsigned>(blocks), 256, 0, s>>>(in, n, reinterpret_cast<uint32_t*>(*out));
+    note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "rc_compress_kernel");
     return QDB_OK;

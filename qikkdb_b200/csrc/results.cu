@@ -301,7 +301,9 @@ int32_t qdb_gb_results_multi(qdb_gb* gb, int32_t n_aggs, const int32_t* aggs, vo
         return rc;
     }
     res_count_kernel<<<static_cast<unsigned>(nchunks), kResThreads, 0, s>>>(sp, counts);
+    note_launch();
     res_scan_kernel<<<1, kResThreads, 0, s>>>(counts, nchunks, d_total);
+    note_launch();
     long long total = 0;
     cudaError_t e = cudaMemcpyAsync(&total, d_total, sizeof(total), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -366,6 +368,7 @@ int32_t qdb_gb_results_multi(qdb_gb* gb, int32_t n_aggs, const int32_t* aggs, vo
     if (out_val_nulls)
         for (int i = 0; i < n_aggs; ++i) cudaMemsetAsync(out_val_nulls[i], 0, nwords * 8, s);
     res_emit_kernel<<<static_cast<unsigned>(nchunks), kResThreads, 0, s>>>(ea);
+    note_launch();
     e = cudaGetLastError();
     dev_free(counts, s);
     dev_free(d_total, s);

@@ -4,6 +4,7 @@
 // qikkDB/QueryEngine/GPUCore/GPUMemory.cuh:89-236, qikkDB/QueryEngine/CudaMemAllocator.h:11-60):
 // instead of a best-fit allocator over one reserved block, device memory comes from CUDA's
 // stream-ordered pool with its release threshold raised so freed blocks are reused.
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -12,6 +13,9 @@
 namespace qdb {
 
 static thread_local std::string g_last_error = "";
+static std::atomic<int64_t> g_launches{0};
+
+void note_launch(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
@@ -77,6 +81,8 @@ using namespace qdb;
 extern "C" {
 
 const char* qdb_last_error(void) { return g_last_error.c_str(); }
+
+int64_t qdb_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 const char* qdb_version(void) { return "qikkdb_b200 0.1 (sm_100a)"; }
 

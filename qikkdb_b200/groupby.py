@@ -184,6 +184,7 @@ def make_pred(col: torch.Tensor, op: int, constant, const_dtype=None, nulls: Opt
     else:
         p.const_i = int(constant)
     p.nulls = _ptr(nulls)
+    p._keep = (col, nulls)  # the struct holds raw pointers: keep the tensors alive with it
     return p
 
 
@@ -225,6 +226,44 @@ class GroupByTable:
         fn = capi.lib().qdb_gb_process_sync if sync else capi.lib().qdb_gb_process
         capi.check(fn(self.handle, kc, kn, _ptr(values), _ptr(value_nulls), int(n),
                       C.byref(pred) if pred is not None else None, _ptr(mask), _stream(stream)))
+
+    def process_host(self, keys, values=None, key_nulls=None, value_nulls=None, pred=None, mask=None,
+                     chunk_rows: int = 1 << 24, stream=None) -> None:
+        """qdb_gb_process_host: host (numpy / pinned CPU tensor) columns, streamed to the GPU in chunks.
+        pred: (host column, op, constant, constant dtype[, host null words]).  Asynchronous: the host arrays must
+        stay alive until `stream` has passed this call."""
+        def hp(x):
+            if x is None:
+                return None
+            if isinstance(x, torch.Tensor):
+                assert not x.is_cuda and x.is_contiguous()
+                return x.data_ptr()
+            return np.ascontiguousarray(x).ctypes.data
+        keys = list(keys) if isinstance(keys, (list, tuple)) else [keys]
+        n = len(keys[0])
+        kc = (C.c_void_p * len(keys))(*[hp(k) for k in keys])
+        kn = None
+        if key_nulls is not None:
+            key_nulls = list(key_nulls) if isinstance(key_nulls, (list, tuple)) else [key_nulls]
+            kn = (C.c_void_p * len(key_nulls))(*[hp(k) for k in key_nulls])
+        p = None
+        if pred is not None:
+            col, op, const, cdt = pred[:4]
+            pn = pred[4] if len(pred) > 4 else None
+            p = capi.qdb_pred()
+            p.col = hp(col)
+            p.type = type_code(col.dtype)
+            p.op = op
+            ct = type_code(cdt)
+            p.const_type = ct
+            if ct in (capi.QDB_FLOAT, capi.QDB_DOUBLE):
+                p.const_f = float(np.float32(const)) if ct == capi.QDB_FLOAT else float(const)
+            else:
+                p.const_i = int(const)
+            p.nulls = hp(pn)
+        capi.check(capi.lib().qdb_gb_process_host(self.handle, kc, kn, hp(values), hp(value_nulls), int(n),
+                                                  C.byref(p) if p is not None else None, hp(mask), int(chunk_rows),
+                                                  _stream(stream)))
 
     def check(self, stream=None) -> None:
         capi.check(capi.lib().qdb_gb_check(self.handle, _stream(stream)))

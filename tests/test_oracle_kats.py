@@ -47,9 +47,10 @@ def test_oracle_int_sum_wraps_like_int32_atomics():
     k = np.zeros(3, dtype=np.int32)
     v = np.array([2**31 - 1, 5, 7], dtype=np.int32)
     r = oracle.groupby(k, v, threads=1)
-    assert r["sum"][0] == np.int64(np.int32(np.int64(2**31 - 1 + 12) - 2**32))
-    # AVG divides the wrapped sum (GPUBinary<div> on the int32 sum)
-    assert r["avg"][0] == int(np.int32(np.int64(2**31 - 1 + 12) - 2**32)) // 3 or r["avg"][0] == -((-(int(np.int32(np.int64(2**31 - 1 + 12) - 2**32)))) // 3)
+    wrapped = (2**31 - 1 + 12) - 2**32  # int32 two's-complement wrap
+    assert r["sum"][0] == wrapped
+    # AVG divides the wrapped sum with C++ truncation toward zero (GPUBinary<div> on the int32 sum)
+    assert r["avg"][0] == int(wrapped / 3)
 
 
 def test_oracle_filter_and_compaction():
