@@ -396,7 +396,9 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     const size_t stage_area = a.staged ? static_cast<size_t>(NS) * sl.bytes : 0;
     const size_t bar_bytes = 128;
     const size_t list_bytes = (static_cast<size_t>(T) * 2 + 127) & ~size_t(127);
-    const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes;
+    const size_t queue_bytes = static_cast<size_t>(kConsumerWarps) * kQueueCap * (8 + 8 + 4);
+    const size_t budget =
+        static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes - queue_bytes;
 
     // Shared-memory hash table sizing.
     size_t hash_bytes = 0;
@@ -414,7 +416,7 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
             const size_t S2 = S + 2;
             a.S = S;
             a.probe = (static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2)
-                          ? S : static_cast<int>(env_int("QDB_AGG_PROBE", 16));
+                          ? S : static_cast<int>(env_int("QDB_AGG_PROBE", 4));
             size_t off = S2 * 8;
             if (a.has_sum) { a.so_sum = static_cast<int32_t>(off); off += S2 * 8; }
             if (has_mm) {
@@ -430,8 +432,9 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     }
     a.so_bar = static_cast<int32_t>(hash_bytes);
     a.so_list = static_cast<int32_t>(hash_bytes + bar_bytes);
-    a.so_stage = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes);
-    const size_t smem = hash_bytes + bar_bytes + list_bytes + stage_area;
+    a.so_queue = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes);
+    a.so_stage = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes + ((queue_bytes + 127) & ~size_t(127)));
+    const size_t smem = a.so_stage + stage_area;
     return launch_agg(gb, a, ptype, nulls, smem, s);
 }
 

@@ -12,7 +12,9 @@
 //       - first into a per-CTA shared-memory table (bounded linear probe, shared-memory atomics), which
 //         absorbs low-cardinality and skewed (Zipf) key streams,
 //       - on a miss, into the global open-addressing table (bounded linear probe, 64-bit atomicCAS on the
-//         key word, fire-and-forget reductions on the state words);
+//         key word, fire-and-forget reductions on the state words).  Misses are queued per warp and
+//         inserted 32 at a time in two phases (probe load issued, finished one batch later), so the L2
+//         round trips overlap other work;
 //     then release the stage to the producer.  No mask or compacted column is written to HBM.
 // A warp that sees a low shared-memory hit rate after its first tiles stops probing shared memory.
 // At the end each CTA merges its shared-memory table into the global table.
@@ -27,6 +29,7 @@ constexpr int kConsumerWarps = 30;
 constexpr int kConsumerThreads = kConsumerWarps * 32;     // 960
 constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer warp: 992 threads
 constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsumerWarps * R rows, R a multiple of 64
+constexpr int kQueueCap = 64;                              // per-warp queue of shared-memory misses
 constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
 constexpr uint32_t kMaxWaitIters = 1u << 24;               // bounded mbarrier waits (seconds, then give up)
 
@@ -73,7 +76,7 @@ struct AggArgs {
     int32_t S = 0;       // shared-memory hash slots (power of two) or 0 for a global-only pass
     int32_t probe = 0;   // shared-memory probe limit
     // byte offsets inside dynamic shared memory
-    int32_t so_stage = 0, so_bar = 0, so_list = 0;
+    int32_t so_stage = 0, so_bar = 0, so_list = 0, so_queue = 0;
     int32_t so_sum = 0, so_mn = 0, so_mx = 0, so_cnt = 0;  // hash arrays (keys at offset 0), S + 2 entries each
 };
 
@@ -173,10 +176,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsign
     atomicExch(reinterpret_cast<int*>(&counters[1]), static_cast<int>(QDB_ERR_TIMEOUT));
     return false;
 }
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// L2 policy for data read once: evict first, so the column stream does not push the hash table out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
         : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async_smem() {
@@ -402,6 +412,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         // ---------------- producer warp: one elected lane issues the bulk copies ----------------
         if (lane == 0 && a.staged) {
             const StageLayout& sl = a.sl;
+            const uint64_t pol = l2_evict_first_policy();
             int64_t q = 0;
             for (; q < my_tiles; ++q) {
                 const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
@@ -419,15 +430,15 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 tx += words * ((sl.knull0 >= 0) + (sl.knull1 >= 0) + (sl.vnull >= 0) + (sl.pnull >= 0));
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full_bar[s], tx);
-                bulk_g2s(st + sl.key0, static_cast<const KT*>(a.key0) + r0, T * sizeof(KT), &full_bar[s]);
-                if (COMP) bulk_g2s(st + sl.key1, static_cast<const KT*>(a.key1) + r0, T * sizeof(KT), &full_bar[s]);
-                if (sl.val >= 0) bulk_g2s(st + sl.val, static_cast<const VT*>(a.vals) + r0, T * sizeof(VT), &full_bar[s]);
-                if (sl.pred >= 0) bulk_g2s(st + sl.pred, static_cast<const PL*>(a.pcol) + r0, T * sizeof(PL), &full_bar[s]);
-                if (sl.mask >= 0) bulk_g2s(st + sl.mask, a.mask + r0, T, &full_bar[s]);
-                if (sl.knull0 >= 0) bulk_g2s(st + sl.knull0, a.knull0 + r0 / 64, words, &full_bar[s]);
-                if (sl.knull1 >= 0) bulk_g2s(st + sl.knull1, a.knull1 + r0 / 64, words, &full_bar[s]);
-                if (sl.vnull >= 0) bulk_g2s(st + sl.vnull, a.vnull + r0 / 64, words, &full_bar[s]);
-                if (sl.pnull >= 0) bulk_g2s(st + sl.pnull, a.pnull + r0 / 64, words, &full_bar[s]);
+                bulk_g2s(st + sl.key0, static_cast<const KT*>(a.key0) + r0, T * sizeof(KT), &full_bar[s], pol);
+                if (COMP) bulk_g2s(st + sl.key1, static_cast<const KT*>(a.key1) + r0, T * sizeof(KT), &full_bar[s], pol);
+                if (sl.val >= 0) bulk_g2s(st + sl.val, static_cast<const VT*>(a.vals) + r0, T * sizeof(VT), &full_bar[s], pol);
+                if (sl.pred >= 0) bulk_g2s(st + sl.pred, static_cast<const PL*>(a.pcol) + r0, T * sizeof(PL), &full_bar[s], pol);
+                if (sl.mask >= 0) bulk_g2s(st + sl.mask, a.mask + r0, T, &full_bar[s], pol);
+                if (sl.knull0 >= 0) bulk_g2s(st + sl.knull0, a.knull0 + r0 / 64, words, &full_bar[s], pol);
+                if (sl.knull1 >= 0) bulk_g2s(st + sl.knull1, a.knull1 + r0 / 64, words, &full_bar[s], pol);
+                if (sl.vnull >= 0) bulk_g2s(st + sl.vnull, a.vnull + r0 / 64, words, &full_bar[s], pol);
+                if (sl.pnull >= 0) bulk_g2s(st + sl.pnull, a.pnull + r0 / 64, words, &full_bar[s], pol);
             }
             // Drain: every issued stage must have been consumed (so no copy is still in flight) before exit.
             for (int64_t d = (q > a.NS ? q - a.NS : 0); d < q; ++d) {
@@ -450,6 +461,51 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         uint16_t* list = reinterpret_cast<uint16_t*>(sm + a.so_list) + warp * R;
         const uint32_t lt_mask = (1u << lane) - 1u;
         const int smem_shift = 32 - (31 - __clz(S > 0 ? S : 1));
+        // Per-warp queue of shared-memory misses (raw rows: key word, value bits, kind | agg flag).
+        uint64_t* qkw = reinterpret_cast<uint64_t*>(sm + a.so_queue) + warp * kQueueCap;
+        uint64_t* qval = reinterpret_cast<uint64_t*>(sm + a.so_queue) + (kConsumerWarps + warp) * kQueueCap;
+        uint32_t* qmeta = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(sm + a.so_queue) +
+                                                      2 * kConsumerWarps * kQueueCap) + warp * kQueueCap;
+        int qn = 0;
+        // Global inserts are split in two phases so their L2 round trip overlaps a tile of other work:
+        // `issue` pops queue entry e into this lane's registers and issues the first probe load;
+        // `complete` (called one batch later) finishes the probe and applies the reductions.
+        bool pf = false;
+        uint64_t pf_kw = 0, pf_val = 0, pf_word = 0, pf_s = 0;
+        uint32_t pf_meta = 0;
+        auto issue = [&](int e) {
+            pf_kw = qkw[e];
+            pf_val = qval[e];
+            pf_meta = qmeta[e];
+            pf = true;
+            const int kind = static_cast<int>(pf_meta & 3u);
+            if (kind == KK_NORMAL || kind == KK_AUX) {
+                const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
+                pf_s = mix64(pf_kw) & Rg.mask;
+                pf_word = ld_volatile_u64(Rg.slots + pf_s * W);
+            }
+        };
+        auto complete = [&]() {
+            if (!pf) return;
+            pf = false;
+            const int kind = static_cast<int>(pf_meta & 3u);
+            uint64_t* slot;
+            if (kind == KK_NORMAL || kind == KK_AUX) {
+                const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
+                slot = g_find_from(Rg, W, pf_kw, pf_s, pf_word, a.counters, a.capacity);
+            } else {
+                slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, a.counters, a.capacity);
+            }
+            if (slot && (pf_meta & 4u)) {
+                if (has_vals) {
+                    VT v;
+                    memcpy(&v, &pf_val, sizeof(VT));
+                    g_acc_row<VT>(slot, a, v);
+                } else {
+                    g_count_row(slot, a.L);
+                }
+            }
+        };
         for (int64_t q = 0; q < my_tiles; ++q) {
             const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
             const bool staged = a.staged && tile < a.full_tiles;
@@ -484,56 +540,63 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 count += __popc(b);
             }
             __syncwarp();
-            // Phase B: insert the passing rows.
-            for (int e = lane; e < count; e += 32) {
-                const int i = list[e];
-                const int64_t r = base + i;
-                KT k0, k1 = KT{};
+            // Phase B: insert the passing rows into the shared-memory table; rows that miss it are queued
+            // and inserted into the global table 32 at a time, so the L2 round trips of a warp overlap.
+            for (int e0 = 0; e0 < count; e0 += 32) {
+                const int e = e0 + lane;
+                const bool act = e < count;
+                uint64_t kw = 0;
+                int kind = KK_NORMAL;
+                bool agg_it = false;
                 VT v = VT{};
-                bool kn0 = false, kn1 = false, vn = false;
-                if (staged) {
-                    k0 = reinterpret_cast<const KT*>(st + a.sl.key0)[i];
-                    if constexpr (COMP) k1 = reinterpret_cast<const KT*>(st + a.sl.key1)[i];
-                    if (has_vals) v = reinterpret_cast<const VT*>(st + a.sl.val)[i];
-                    if constexpr (NULLS) {
-                        const int wi = i >> 6, bb = i & 63;
-                        if (a.sl.knull0 >= 0) kn0 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull0)[wi] >> bb) & 1;
-                        if (a.sl.knull1 >= 0) kn1 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull1)[wi] >> bb) & 1;
-                        if (a.sl.vnull >= 0) vn = (reinterpret_cast<const uint64_t*>(st + a.sl.vnull)[wi] >> bb) & 1;
-                    }
-                } else {
-                    k0 = static_cast<const KT*>(a.key0)[r];
-                    if constexpr (COMP) k1 = static_cast<const KT*>(a.key1)[r];
-                    if (has_vals) v = static_cast<const VT*>(a.vals)[r];
-                    if constexpr (NULLS) {
-                        kn0 = null_bit(a.knull0, r);
-                        kn1 = null_bit(a.knull1, r);
-                        vn = null_bit(a.vnull, r);
-                    }
-                }
-                uint64_t kw;
-                int kind;
-                if constexpr (COMP) {
-                    if (kn0 || kn1) {
-                        kind = KK_AUX;
-                        const uint32_t other = kn0 ? (kn1 ? 0u : static_cast<uint32_t>(k1)) : static_cast<uint32_t>(k0);
-                        kw = (static_cast<uint64_t>((kn0 ? 1u : 0u) | (kn1 ? 2u : 0u)) << 32) | other;
+                if (act) {
+                    const int i = list[e];
+                    const int64_t r = base + i;
+                    KT k0, k1 = KT{};
+                    bool kn0 = false, kn1 = false, vn = false;
+                    if (staged) {
+                        k0 = reinterpret_cast<const KT*>(st + a.sl.key0)[i];
+                        if constexpr (COMP) k1 = reinterpret_cast<const KT*>(st + a.sl.key1)[i];
+                        if (has_vals) v = reinterpret_cast<const VT*>(st + a.sl.val)[i];
+                        if constexpr (NULLS) {
+                            const int wi = i >> 6, bb = i & 63;
+                            if (a.sl.knull0 >= 0) kn0 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull0)[wi] >> bb) & 1;
+                            if (a.sl.knull1 >= 0) kn1 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull1)[wi] >> bb) & 1;
+                            if (a.sl.vnull >= 0) vn = (reinterpret_cast<const uint64_t*>(st + a.sl.vnull)[wi] >> bb) & 1;
+                        }
                     } else {
-                        kw = composite_word(static_cast<int32_t>(k0), static_cast<int32_t>(k1));
-                        kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                        k0 = static_cast<const KT*>(a.key0)[r];
+                        if constexpr (COMP) k1 = static_cast<const KT*>(a.key1)[r];
+                        if (has_vals) v = static_cast<const VT*>(a.vals)[r];
+                        if constexpr (NULLS) {
+                            kn0 = null_bit(a.knull0, r);
+                            kn1 = null_bit(a.knull1, r);
+                            vn = null_bit(a.vnull, r);
+                        }
                     }
-                } else {
-                    if (kn0) {
-                        kind = KK_NULL;
-                        kw = 0;
+                    if constexpr (COMP) {
+                        if (kn0 || kn1) {
+                            kind = KK_AUX;
+                            const uint32_t other =
+                                kn0 ? (kn1 ? 0u : static_cast<uint32_t>(k1)) : static_cast<uint32_t>(k0);
+                            kw = (static_cast<uint64_t>((kn0 ? 1u : 0u) | (kn1 ? 2u : 0u)) << 32) | other;
+                        } else {
+                            kw = composite_word(static_cast<int32_t>(k0), static_cast<int32_t>(k1));
+                            kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                        }
                     } else {
-                        kw = key_word(k0);
-                        kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                        if (kn0) {
+                            kind = KK_NULL;
+                        } else {
+                            kw = key_word(k0);
+                            kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                        }
                     }
+                    agg_it = !has_vals || !vn;
                 }
-                const bool agg_it = !has_vals || !vn;
-                int slot_s = -1;
-                if (use_smem && kind != KK_AUX) {
+                bool miss = act;
+                if (act && use_smem && kind != KK_AUX) {
+                    int slot_s;
                     if (kind == KK_NORMAL) {
                         bool found = false;
                         slot_s = s_find(skey, S, a.probe, kw, smem_hash(kw, smem_shift), &found);
@@ -544,21 +607,27 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                         if (*reinterpret_cast<volatile uint64_t*>(&skey[slot_s]) == kEmpty)
                             atomicCAS(reinterpret_cast<unsigned long long*>(&skey[slot_s]), kEmpty, 0ull);
                     }
+                    if (slot_s >= 0) {
+                        miss = false;
+                        if (agg_it) s_acc_row<VT>(sm, a, slot_s, v, has_vals);
+                    }
                 }
-                if (slot_s >= 0) {
-                    if (agg_it) s_acc_row<VT>(sm, a, slot_s, v, has_vals);
-                    continue;
+                const uint32_t mb = __ballot_sync(0xffffffffu, miss);
+                if (miss) {
+                    const int pos = qn + __popc(mb & lt_mask);
+                    qkw[pos] = kw;
+                    uint64_t vb = 0;
+                    memcpy(&vb, &v, sizeof(VT));
+                    qval[pos] = vb;
+                    qmeta[pos] = static_cast<uint32_t>(kind) | (agg_it ? 4u : 0u);
                 }
-                uint64_t* slot;
-                if (kind == KK_NORMAL || kind == KK_AUX) {
-                    const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
-                    slot = g_find(Rg, W, kw, mix64(kw), a.counters, a.capacity);
-                } else {
-                    slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, a.counters, a.capacity);
-                }
-                if (slot && agg_it) {
-                    if (has_vals) g_acc_row<VT>(slot, a, v);
-                    else g_count_row(slot, a.L);
+                qn += __popc(mb);
+                if (qn >= 32) {
+                    __syncwarp();
+                    complete();
+                    qn -= 32;
+                    issue(qn + lane);
+                    __syncwarp();
                 }
             }
             if (staged) {
@@ -572,6 +641,13 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             }
             __syncwarp();
         }
+        __syncwarp();
+        complete();
+        if (lane < qn) {
+            issue(lane);
+            complete();
+        }
+        __syncwarp();
     }
 
     // Merge this CTA's shared-memory table into the global table.
