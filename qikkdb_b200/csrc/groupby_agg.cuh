@@ -13,8 +13,7 @@
 //         absorbs low-cardinality and skewed (Zipf) key streams,
 //       - on a miss, into the global open-addressing table (bounded linear probe, 64-bit atomicCAS on the
 //         key word, fire-and-forget reductions on the state words).  Misses are queued per warp and
-//         inserted 32 at a time in two phases (probe load issued, finished one batch later), so the L2
-//         round trips overlap other work;
+//         inserted 32 at a time with every lane active, so 32 probe loads of a warp are in flight together;
 //     then release the stage to the producer.  No mask or compacted column is written to HBM.
 // A warp that sees a low shared-memory hit rate after its first tiles stops probing shared memory.
 // At the end each CTA merges its shared-memory table into the global table.
@@ -467,9 +466,10 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         uint32_t* qmeta = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(sm + a.so_queue) +
                                                       2 * kConsumerWarps * kQueueCap) + warp * kQueueCap;
         int qn = 0;
-        // Global inserts are split in two phases so their L2 round trip overlaps a tile of other work:
-        // `issue` pops queue entry e into this lane's registers and issues the first probe load;
-        // `complete` (called one batch later) finishes the probe and applies the reductions.
+        // Global inserts of queued misses: `issue` pops queue entry e into this lane's registers and issues the
+        // first probe load; `complete` finishes the probe and applies the reductions.  A whole warp drains 32
+        // entries at once, so 32 probe loads are in flight together.  (Deferring `complete` by one batch to
+        // overlap the round trip with the next tile measured slower.)
         bool pf = false;
         uint64_t pf_kw = 0, pf_val = 0, pf_word = 0, pf_s = 0;
         uint32_t pf_meta = 0;
@@ -624,9 +624,9 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 qn += __popc(mb);
                 if (qn >= 32) {
                     __syncwarp();
-                    complete();
                     qn -= 32;
                     issue(qn + lane);
+                    complete();
                     __syncwarp();
                 }
             }
