@@ -204,6 +204,22 @@ int32_t qdb_filter(int32_t op, int32_t a_type, int32_t a_is_col, const void* a, 
 int32_t qdb_reconstruct_keep(int32_t elem_bytes, const void* in, const int8_t* mask, int64_t n, void** out,
                              int64_t* out_count, const uint64_t* null_in, uint64_t** out_null_mask,
                              void* stream);
+/* Compaction that allocates nothing.  No counterpart in the reference: it exists for callers that own all
+ * device memory themselves (a buffer pool that accounts every byte of HBM, a serving loop admitting queries
+ * against a fixed HBM budget) and so cannot let a library call cudaMalloc or cudaFree during a query: such an
+ * allocation can fail mid-query under their memory pressure, escapes their accounting, and cudaFree
+ * synchronises the device.  Same selection as qdb_reconstruct_keep (mask required), but the caller passes
+ * the output buffer `out` (room for out_capacity elements of elem_bytes) and, when null_in is given, an
+ * output null mask with room for ceil(out_capacity / 64) words; *out_count receives the number of selected
+ * rows (the call synchronises `stream` to read it).  Selecting more than out_capacity rows returns
+ * QDB_ERR_TOO_LARGE and writes nothing.  Limit: n <= 268435456 (2^28) rows, else QDB_ERR_TOO_LARGE.
+ * Scratch is a fixed 512 KiB array that the library holds on every GPU that loads it until the process
+ * exits; the first call on a device looks up that array's device address, so make the first call before
+ * any stream capture.  All calls on a device share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
+int32_t qdb_reconstruct_keep_noalloc(int32_t elem_bytes, const void* in, const int8_t* mask, int64_t n, void* out,
+                                     int64_t out_capacity, int64_t* out_count, const uint64_t* null_in,
+                                     uint64_t* out_null_mask, void* stream);
 /* GenerateIndexesKeep<int32_t,int8_t> (GPUReconstruct.cuh:518-566): int32 row indices where mask != 0. */
 int32_t qdb_generate_indexes(const int8_t* mask, int64_t n, int32_t** out, int64_t* out_count, void* stream);
 /* PrefixSum<int32_t,int8_t> (GPUReconstruct.cuh:573-583): inclusive sum of mask into out[n] (caller-owned). */

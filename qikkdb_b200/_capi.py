@@ -86,6 +86,7 @@ SIGNATURES = [
     ("qdb_gb_merge_partial", I32, [P, P, P, P, I64, P]),
     ("qdb_filter", I32, [I32, I32, I32, P, I32, I32, P, P, P, I64, P]),
     ("qdb_reconstruct_keep", I32, [I32, P, P, I64, PP, PI64, P, PP, P]),
+    ("qdb_reconstruct_keep_noalloc", I32, [I32, P, P, I64, P, I64, PI64, P, P, P]),
     ("qdb_generate_indexes", I32, [P, I64, PP, PI64, P]),
     ("qdb_prefix_sum", I32, [P, I64, P, P]),
     ("qdb_compress_null_mask", I32, [P, I64, PP, P]),

@@ -7,6 +7,8 @@
 // the selected rows of every 4096-row tile (1 B/row read), one block scans the tile counts, and the
 // scatter pass recomputes each thread's offset inside its tile from the mask (a block scan in registers
 // and shared memory), so no per-row prefix array touches HBM.  No pass waits on another CTA.
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "qdb_common.cuh"
@@ -337,3 +339,95 @@ int32_t qdb_compress_null_mask(const uint8_t* in, int64_t n, uint64_t** out, voi
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Compaction without any allocation, for callers that may not allocate device memory.
+//
+// Some callers own every byte of device memory themselves: a database buffer pool that accounts all
+// HBM, or a serving loop that admits queries against a fixed HBM budget.  They cannot let a library
+// call cudaMalloc behind their back: the allocation can fail in the middle of a query under their
+// memory pressure, escapes their accounting, and cudaFree synchronises the whole device.  This entry
+// point therefore works only in memory the caller passes in plus one fixed scratch array that the
+// library holds for the life of the process on every GPU that loads it.
+// ---------------------------------------------------------------------------------------------
+namespace qdb {
+
+// Largest input the no-allocation compaction accepts: kNoAllocMaxTiles tiles of kRcTile rows (2^28 rows).
+constexpr int64_t kNoAllocMaxTiles = 65536;
+constexpr int64_t kNoAllocMaxRows = kNoAllocMaxTiles * kRcTile;
+
+// Per-tile counts and offsets (+ the total in the last entry): 512 KiB + 8 bytes per GPU, allocated when
+// the library is loaded and kept until the process exits.  Shared by every call on the device.
+static __device__ __align__(256) long long g_noalloc_tile_offsets[kNoAllocMaxTiles + 1];
+
+// Device address of g_noalloc_tile_offsets on each device.  In host code the symbol is only a host-side
+// stand-in, so the address must be looked up with the device current.
+static std::mutex g_noalloc_mu;
+static std::vector<long long*> g_noalloc_ptr;
+
+static int32_t noalloc_scratch(long long** out) {
+    int dev = 0;
+    QDB_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (static_cast<int>(g_noalloc_ptr.size()) <= dev) g_noalloc_ptr.resize(dev + 1, nullptr);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tile_offsets);
+        if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_tile_offsets)");
+        g_noalloc_ptr[dev] = static_cast<long long*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return QDB_OK;
+}
+
+}  // namespace qdb
+
+extern "C" int32_t qdb_reconstruct_keep_noalloc(int32_t elem_bytes, const void* in, const int8_t* mask, int64_t n,
+                                                void* out, int64_t out_capacity, int64_t* out_count,
+                                                const uint64_t* null_in, uint64_t* out_null_mask, void* stream) {
+    if (!out_count) return fail(QDB_ERR_INVALID, "qdb_reconstruct_keep_noalloc: null out_count");
+    *out_count = 0;
+    if (elem_bytes != 1 && elem_bytes != 2 && elem_bytes != 4 && elem_bytes != 8)
+        return fail(QDB_ERR_INVALID, "qdb_reconstruct_keep_noalloc: elem_bytes must be 1, 2, 4 or 8");
+    if (n < 0) return fail(QDB_ERR_INVALID, "qdb_reconstruct_keep_noalloc: negative row count");
+    if (n > kNoAllocMaxRows)
+        return fail(QDB_ERR_TOO_LARGE, "qdb_reconstruct_keep_noalloc: at most 268435456 rows per call (n = " +
+                                           std::to_string(n) + ")");
+    if (n == 0) return QDB_OK;
+    if (!in || !mask || (!out && out_capacity > 0))
+        return fail(QDB_ERR_INVALID, "qdb_reconstruct_keep_noalloc: null input, mask or output");
+    long long* offs = nullptr;
+    int32_t rc = noalloc_scratch(&offs);
+    if (rc != QDB_OK) return rc;
+    cudaStream_t s = as_stream(stream);
+    const int64_t ntiles = (n + kRcTile - 1) / kRcTile;
+    const int vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0;
+    // Every entry the scan reads is written by the count pass first, so the scratch needs no clearing.
+    rc_count_kernel<<<static_cast<unsigned>(ntiles), kRcThreads, 0, s>>>(mask, n, vec, offs);
+    note_launch();
+    rc_scan_kernel<<<1, kRcThreads, 0, s>>>(offs, ntiles);
+    note_launch();
+    long long total = 0;
+    cudaError_t e = cudaMemcpyAsync(&total, offs + ntiles, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "qdb_reconstruct_keep_noalloc: count pass");
+    if (total > out_capacity)
+        return fail(QDB_ERR_TOO_LARGE, "qdb_reconstruct_keep_noalloc: " + std::to_string(total) +
+                                           " selected rows exceed out_capacity " + std::to_string(out_capacity));
+    if (total == 0) return QDB_OK;
+    unsigned long long* nout = nullptr;
+    if (null_in && out_null_mask) {
+        nout = reinterpret_cast<unsigned long long*>(out_null_mask);
+        QDB_CUDA_TRY(cudaMemsetAsync(nout, 0, ((static_cast<size_t>(total) + 63) / 64) * 8, s));
+    }
+    switch (elem_bytes) {
+        case 1: launch_scatter<uint8_t>(in, mask, n, offs, out, null_in, nout, s); break;
+        case 2: launch_scatter<uint16_t>(in, mask, n, offs, out, null_in, nout, s); break;
+        case 4: launch_scatter<uint32_t>(in, mask, n, offs, out, null_in, nout, s); break;
+        default: launch_scatter<uint64_t>(in, mask, n, offs, out, null_in, nout, s); break;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "rc_scatter_kernel (no-allocation form)");
+    *out_count = total;
+    return QDB_OK;
+}
