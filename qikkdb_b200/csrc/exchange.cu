@@ -60,15 +60,18 @@ __global__ void merge_partial_kernel(Region main, Region aux, Layout L, int32_t 
                                      const uint64_t* state, const uint8_t* flags, int64_t n,
                                      unsigned long long* counters, unsigned long long capacity) {
     const int sw = L.W - 1;
+    __shared__ unsigned long long s_claims;
+    if (threadIdx.x == 0) s_claims = 0;
+    __syncthreads();
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const uint8_t f = flags[i];
         const uint64_t kw = keys[i];
         uint64_t* slot;
-        if (f & EX_NULL_KEY) slot = g_special(main, L.W, 0, counters, capacity);
-        else if (f & EX_ESCAPE_KEY) slot = g_special(main, L.W, 1, counters, capacity);
-        else if (f & EX_AUX_KEY) slot = aux.slots ? g_find(aux, L.W, kw, mix64(kw), counters, capacity) : nullptr;
-        else slot = g_find(main, L.W, kw, mix64(kw), counters, capacity);
+        if (f & EX_NULL_KEY) slot = g_special(main, L.W, 0, &s_claims);
+        else if (f & EX_ESCAPE_KEY) slot = g_special(main, L.W, 1, &s_claims);
+        else if (f & EX_AUX_KEY) slot = aux.slots ? g_find(aux, L.W, kw, mix64(kw), counters, &s_claims) : nullptr;
+        else slot = g_find(main, L.W, kw, mix64(kw), counters, &s_claims);
         if (!slot || sw == 0) continue;
         const uint64_t* st = state + i * sw;
         const unsigned long long c = (L.cnt >= 0) ? st[L.cnt - 1] : 0ull;
@@ -88,6 +91,8 @@ __global__ void merge_partial_kernel(Region main, Region aux, Layout L, int32_t 
             g_merge(slot, L, has_sum, has_min, has_max, v32, vfloat, c, sumbits, mn, mx);
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0) publish_claims(counters, capacity, s_claims);
 }
 
 }  // namespace qdb

@@ -206,8 +206,15 @@ __device__ __forceinline__ long long enc64(VT v) {
     else return static_cast<long long>(v);
 }
 
-__device__ __forceinline__ void claim_counted(unsigned long long* counters, unsigned long long capacity) {
-    if (atomicAdd(&counters[0], 1ull) >= capacity)
+// New groups are counted in a per-CTA shared-memory counter (a single global counter hit by every new
+// key would serialise in L2); each CTA publishes its count once with publish_claims, which raises
+// HASH_TABLE_FULL when the total passes the capacity.
+__device__ __forceinline__ void claim_counted(unsigned long long* claims) { atomicAdd(claims, 1ull); }
+
+__device__ __forceinline__ void publish_claims(unsigned long long* counters, unsigned long long capacity,
+                                               unsigned long long claims) {
+    if (claims == 0) return;
+    if (atomicAdd(&counters[0], claims) + claims > capacity)
         atomicExch(reinterpret_cast<int*>(&counters[1]), static_cast<int>(QDB_HASH_TABLE_FULL));
 }
 
@@ -219,7 +226,7 @@ __device__ __forceinline__ bool table_full(const unsigned long long* counters) {
 // The probe visits at most every slot once, so it always ends; it gives up (returns nullptr) when the
 // region is full or another thread has already reported HASH_TABLE_FULL.
 __device__ __forceinline__ uint64_t* g_find_from(const Region& R, int W, uint64_t key, uint64_t s, uint64_t cur,
-                                                 unsigned long long* counters, unsigned long long capacity) {
+                                                 unsigned long long* counters, unsigned long long* claims) {
     for (uint64_t i = 0; i <= R.mask; ++i) {
         uint64_t* slot = R.slots + s * W;
         if (i > 0) cur = ld_volatile_u64(slot);
@@ -227,7 +234,7 @@ __device__ __forceinline__ uint64_t* g_find_from(const Region& R, int W, uint64_
         if (cur == kEmpty) {
             unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(slot), kEmpty, key);
             if (prev == kEmpty) {
-                claim_counted(counters, capacity);
+                claim_counted(claims);
                 return slot;
             }
             if (prev == key) return slot;
@@ -240,18 +247,17 @@ __device__ __forceinline__ uint64_t* g_find_from(const Region& R, int W, uint64_
 }
 
 __device__ __forceinline__ uint64_t* g_find(const Region& R, int W, uint64_t key, uint64_t h,
-                                            unsigned long long* counters, unsigned long long capacity) {
+                                            unsigned long long* counters, unsigned long long* claims) {
     const uint64_t s = h & R.mask;
-    return g_find_from(R, W, key, s, ld_volatile_u64(R.slots + s * W), counters, capacity);
+    return g_find_from(R, W, key, s, ld_volatile_u64(R.slots + s * W), counters, claims);
 }
 
 // Special slot `which` (0: NULL key, 1: the key equal to kEmpty) of the main region.
-__device__ __forceinline__ uint64_t* g_special(const Region& R, int W, int which, unsigned long long* counters,
-                                               unsigned long long capacity) {
+__device__ __forceinline__ uint64_t* g_special(const Region& R, int W, int which, unsigned long long* claims) {
     uint64_t* slot = R.slots + (R.mask + 1 + which) * W;
     if (ld_volatile_u64(slot) == kEmpty) {
         unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(slot), kEmpty, 0ull);
-        if (prev == kEmpty && which == 1) claim_counted(counters, capacity);
+        if (prev == kEmpty && which == 1) claim_counted(claims);
     }
     return slot;
 }
@@ -368,6 +374,7 @@ __device__ __forceinline__ void s_acc_row(unsigned char* sm, const AggArgs& a, i
 template <typename KT, bool COMP, typename VT, typename PT, bool NULLS>
 __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ unsigned long long s_claims;
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
 
@@ -393,6 +400,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             }
         }
     }
+    if (threadIdx.x == 0) s_claims = 0;
     if (threadIdx.x == 0 && a.staged) {
         for (int s = 0; s < a.NS; ++s) {
             mbar_init(&full_bar[s], 1);
@@ -492,9 +500,9 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             uint64_t* slot;
             if (kind == KK_NORMAL || kind == KK_AUX) {
                 const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
-                slot = g_find_from(Rg, W, pf_kw, pf_s, pf_word, a.counters, a.capacity);
+                slot = g_find_from(Rg, W, pf_kw, pf_s, pf_word, a.counters, &s_claims);
             } else {
-                slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, a.counters, a.capacity);
+                slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, &s_claims);
             }
             if (slot && (pf_meta & 4u)) {
                 if (has_vals) {
@@ -658,8 +666,8 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         for (int i = threadIdx.x; i < S2; i += blockDim.x) {
             const uint64_t key = skey[i];
             if (key == kEmpty) continue;
-            uint64_t* slot = (i < S) ? g_find(a.main, W, key, mix64(key), a.counters, a.capacity)
-                                     : g_special(a.main, W, i - S, a.counters, a.capacity);
+            uint64_t* slot = (i < S) ? g_find(a.main, W, key, mix64(key), a.counters, &s_claims)
+                                     : g_special(a.main, W, i - S, &s_claims);
             if (!slot) continue;
             const unsigned long long c = reinterpret_cast<unsigned int*>(sm + a.so_cnt)[i];
             const uint64_t sumbits = a.has_sum ? reinterpret_cast<unsigned long long*>(sm + a.so_sum)[i] : 0ull;
@@ -677,6 +685,8 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             g_merge(slot, a.L, a.has_sum, a.has_min, a.has_max, v32, vfloat, c, sumbits, mn, mx);
         }
     }
+    __syncthreads();
+    if (threadIdx.x == 0) publish_claims(a.counters, a.capacity, s_claims);
 }
 
 // Launches the kernel for one type combination: one persistent CTA per SM.
