@@ -20,6 +20,8 @@
 // Every wait on an mbarrier is bounded; a wait that gives up records QDB_ERR_TIMEOUT in the table status.
 #pragma once
 
+#include <climits>
+
 #include "groupby.cuh"
 
 namespace qdb {
@@ -366,6 +368,43 @@ __device__ __forceinline__ void s_acc_row(unsigned char* sm, const AggArgs& a, i
     }
 }
 
+// Register accumulation helpers: the running sum of a group of rows (FP64 for float values, wrapping int64 for
+// integer values) and the order-preserving MIN/MAX encoding.
+template <typename VT>
+using AccOf = typename std::conditional<std::is_floating_point<VT>::value, double, long long>::type;
+
+template <typename VT>
+__device__ __forceinline__ AccOf<VT> to_acc(VT v) {
+    return static_cast<AccOf<VT>>(v);
+}
+
+template <typename VT>
+__device__ __forceinline__ long long enc_any(VT v) {
+    if constexpr (sizeof(VT) == 4) return enc32(v);
+    else return enc64(v);
+}
+
+// Merges c rows with sum `acc` and encoded min/max into shared slot s.
+template <typename VT>
+__device__ __forceinline__ void s_merge_acc(unsigned char* sm, const AggArgs& a, int s, unsigned c, AccOf<VT> acc,
+                                            long long mn, long long mx, bool has_val) {
+    atomicAdd(reinterpret_cast<unsigned int*>(sm + a.so_cnt) + s, c);
+    if (!has_val) return;
+    if (a.has_sum) {
+        if constexpr (std::is_floating_point<VT>::value)
+            atomicAdd(reinterpret_cast<double*>(sm + a.so_sum) + s, acc);
+        else
+            atomicAdd(reinterpret_cast<unsigned long long*>(sm + a.so_sum) + s, static_cast<unsigned long long>(acc));
+    }
+    if constexpr (sizeof(VT) == 4) {
+        if (a.has_min) atomicMin(reinterpret_cast<int*>(sm + a.so_mn) + 2 * s, static_cast<int>(mn));
+        if (a.has_max) atomicMax(reinterpret_cast<int*>(sm + a.so_mx) + 2 * s + 1, static_cast<int>(mx));
+    } else {
+        if (a.has_min) atomicMin(reinterpret_cast<long long*>(sm + a.so_mn) + s, mn);
+        if (a.has_max) atomicMax(reinterpret_cast<long long*>(sm + a.so_mx) + s, mx);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type
 // (int32_t when the table has no value column); PT: predicate column type or NoPred; NULLS: some null
@@ -377,6 +416,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
     __shared__ unsigned long long s_claims;
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
+    using AccT = AccOf<VT>;
 
     const int S = a.S;
     const int S2 = S ? S + 2 : 0;
@@ -474,6 +514,51 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         uint32_t* qmeta = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(sm + a.so_queue) +
                                                       2 * kConsumerWarps * kQueueCap) + warp * kQueueCap;
         int qn = 0;
+        // Two hot keys per warp (the CTA's most frequent shared slots after the first tiles) with per-lane
+        // register accumulators.  64-bit shared atomics serialise when many warps update one slot, so a skewed
+        // key stream would otherwise queue on its hottest slots.
+        uint64_t hk0 = kEmpty, hk1 = kEmpty;  // kEmpty never equals a NORMAL key word
+        unsigned hc0 = 0, hc1 = 0;
+        AccT ha0 = AccT{}, ha1 = AccT{};
+        long long hmn0 = LLONG_MAX, hmx0 = LLONG_MIN, hmn1 = LLONG_MAX, hmx1 = LLONG_MIN;
+        auto pick_hot_keys = [&]() {
+            // warp-wide argmax of the shared slot counts, twice; only keys with a real share of the rows
+            const unsigned* cnt = reinterpret_cast<const unsigned*>(sm + a.so_cnt);
+            unsigned total = 0, b0 = 0, b1 = 0;
+            for (int i = lane; i < S; i += 32) {
+                const unsigned c = cnt[i];
+                total += c;
+                const unsigned key = (min(c, 0x7ffffu) << 13) | static_cast<unsigned>(i & 0x1fff);
+                if (key > b0) {
+                    b1 = b0;
+                    b0 = key;
+                } else if (key > b1) {
+                    b1 = key;
+                }
+            }
+            total = __reduce_add_sync(0xffffffffu, total);
+            const unsigned w0 = __reduce_max_sync(0xffffffffu, b0);
+            const unsigned c0 = (b0 == w0) ? b1 : b0;  // the owner of the first pick offers its runner-up
+            const unsigned w1 = __reduce_max_sync(0xffffffffu, c0);
+            if (S <= 8192 && w0 && (w0 >> 13) * 32u >= total) hk0 = skey[w0 & 0x1fffu];
+            if (S <= 8192 && w1 && (w1 >> 13) * 32u >= total) hk1 = skey[w1 & 0x1fffu];
+            if (hk0 == kEmpty) hk1 = kEmpty;
+        };
+        // Reduces a hot key's per-lane partials over the warp and merges them into the key's shared slot.
+        auto flush_hot = [&](uint64_t hk, unsigned c, AccT acc, long long mn, long long mx) {
+            if (hk == kEmpty) return;
+            for (int o = 16; o > 0; o >>= 1) {
+                c += __shfl_xor_sync(0xffffffffu, c, o);
+                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            if (lane == 0 && c) {
+                bool found = false;
+                const int s = s_find(skey, S, S, hk, smem_hash(hk, smem_shift), &found);
+                if (s >= 0) s_merge_acc<VT>(sm, a, s, c, acc, mn, mx, has_vals);
+            }
+        };
         // Global inserts of queued misses: `issue` pops queue entry e into this lane's registers and issues the
         // first probe load; `complete` finishes the probe and applies the reductions.  A whole warp drains 32
         // entries at once, so 32 probe loads are in flight together.  (Deferring `complete` by one batch to
@@ -603,7 +688,26 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                     agg_it = !has_vals || !vn;
                 }
                 bool miss = act;
-                if (act && use_smem && kind != KK_AUX) {
+                // Rows of the warp's hot keys accumulate in this lane's registers: no probe, no atomic.
+                if (act && kind == KK_NORMAL && (kw == hk0 || kw == hk1)) {
+                    miss = false;
+                    if (agg_it) {
+                        const int j = (kw == hk0) ? 0 : 1;
+                        const AccT x = has_vals ? to_acc<VT>(v) : AccT{};
+                        const long long e = has_vals ? enc_any<VT>(v) : 0;
+                        if (j == 0) {
+                            hc0 += 1;
+                            ha0 += x;
+                            hmn0 = min(hmn0, e);
+                            hmx0 = max(hmx0, e);
+                        } else {
+                            hc1 += 1;
+                            ha1 += x;
+                            hmn1 = min(hmn1, e);
+                            hmx1 = max(hmx1, e);
+                        }
+                    }
+                } else if (act && use_smem && kind != KK_AUX) {
                     int slot_s;
                     if (kind == KK_NORMAL) {
                         bool found = false;
@@ -646,9 +750,12 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 const unsigned hits = __reduce_add_sync(0xffffffffu, my_hits);
                 const unsigned tries = __reduce_add_sync(0xffffffffu, my_tries);
                 if (tries >= 256 && hits * 8u < tries) use_smem = false;
+                else pick_hot_keys();
             }
             __syncwarp();
         }
+        flush_hot(hk0, hc0, ha0, hmn0, hmx0);
+        flush_hot(hk1, hc1, ha1, hmn1, hmx1);
         __syncwarp();
         complete();
         if (lane < qn) {
