@@ -228,6 +228,85 @@ int32_t qdb_prefix_sum(const int8_t* mask, int64_t n, int32_t* out, void* stream
  * (newly allocated, ceil(n/64) words). */
 int32_t qdb_compress_null_mask(const uint8_t* in, int64_t n, uint64_t** out, void* stream);
 
+/* ---- batched GROUP BY: many independent queries in one persistent launch ----
+ * The reference runs one GPUGroupBy per query, each with its own kernel launches and host synchronisations
+ * (GpuSqlDispatcherAggregationFunctions.h:377-507 via GroupByHelper, :99-318).  A batch holds up to
+ * max_instances such queries over device-resident columns and executes all of them with one work-queue-driven
+ * persistent kernel (plus a table-initialisation and a result kernel), optionally replayed as one CUDA graph.
+ * Per query it picks the table placement (shared-memory replicas or the global table), the number of warps that
+ * cooperate on one work item (the effective CTA size) and the rows each thread loads per step, from a tuning
+ * table that qdb_gb_batch_autotune fills by timing candidate plans on the batch's own queries.
+ * Batch instances carry no NULL masks; queries with NULLs use qdb_gb_process. */
+typedef struct qdb_gb_query {
+    int32_t agg_mask;        /* qdb_agg bits; without a value column only QDB_AGG_COUNT */
+    int32_t key_type;        /* QDB_INT32 or QDB_INT64 */
+    int32_t val_type;        /* 0 (no value column) or QDB_INT32 / QDB_INT64 / QDB_FLOAT / QDB_DOUBLE */
+    int32_t reserved;
+    const void* keys;        /* device column of n_rows keys, 16-byte aligned */
+    const void* vals;        /* device column of n_rows values, 16-byte aligned, or NULL when val_type == 0 */
+    int64_t n_rows;
+    int64_t max_groups;      /* distinct-key bound (a cardinality estimate): sizes the table; a query that
+                                exceeds it reports QDB_HASH_TABLE_FULL, as ProcessBlock does */
+    int64_t key_mod;         /* > 0: GROUP BY key % key_mod (C++ remainder, the GPUBinary modulo the dispatcher
+                                would materialise first); 0: GROUP BY key */
+    qdb_pred pred;           /* WHERE col OP constant; pred.col == NULL for none (pred.nulls must be NULL) */
+} qdb_gb_query;
+
+/* Execution plan of one batch instance (what the autotuner chooses). */
+typedef struct qdb_gb_batch_cfg {
+    int32_t placement;       /* QDB_PLACE_SHARED: shared-memory tables merged into the global table at the end of
+                                every work item; QDB_PLACE_GLOBAL: every row goes to the global table */
+    int32_t smem_slots;      /* slots of one shared-memory table (a power of two >= 64), shared placement */
+    int32_t replicas;        /* shared-memory tables per warp group (warp w uses table w % replicas) */
+    int32_t warps;           /* warps cooperating on one work item: 16, 8 or 4 (1, 2 or 4 groups per CTA) */
+    int32_t rows_per_thread; /* rows each thread loads per step: 4 or 8 */
+    int32_t reserved;
+    int64_t chunk_rows;      /* rows per work item (a multiple of 64) */
+} qdb_gb_batch_cfg;
+
+typedef struct qdb_gb_batch qdb_gb_batch; /* opaque batch */
+
+/* Allocates a batch for up to max_instances queries whose hash tables take at most table_bytes of device memory
+ * and whose results take at most result_bytes (per query (max_groups + 2) * (1 + aggregates) * 8 bytes). */
+int32_t qdb_gb_batch_create(qdb_gb_batch** out, int32_t max_instances, int64_t table_bytes, int64_t result_bytes,
+                            void* stream);
+int32_t qdb_gb_batch_destroy(qdb_gb_batch* b);
+/* Replaces the batch's queries and plans them (placement, warps, rows per thread, work items) from the tuning
+ * table; uploads the plan asynchronously.  QDB_ERR_TOO_LARGE when the tables or results do not fit. */
+int32_t qdb_gb_batch_set(qdb_gb_batch* b, const qdb_gb_query* queries, int32_t n, void* stream);
+/* Executes every query of the batch: table initialisation (after a new plan), the persistent aggregation
+ * kernel, and the result kernel (which leaves the tables clean for the next run).  use_graph != 0 replays
+ * one CUDA graph holding the three kernels (captured on first use).  Asynchronous. */
+int32_t qdb_gb_batch_run(qdb_gb_batch* b, int32_t use_graph, void* stream);
+/* Synchronises `stream` and copies every query's group count and status (QDB_OK / QDB_HASH_TABLE_FULL) of the
+ * last run to host arrays of n entries (either may be NULL). */
+int32_t qdb_gb_batch_fetch(qdb_gb_batch* b, int64_t* counts, int32_t* status, void* stream);
+/* Device pointers of query `inst`'s results of the last run, valid until the next run or set: keys[count] as
+ * int64, and one column of count 8-byte words per aggregate of agg_mask in bit order (MIN, MAX, SUM, AVG,
+ * COUNT), column j starting col_stride words after column j - 1: integer results as int64 (the output-type
+ * value sign-extended), float results as double (the output-type value widened exactly).  *n_cols receives
+ * the number of aggregate columns.  The output types are the reference's O: V for MIN/MAX/SUM/AVG, int64 for
+ * COUNT (GpuSqlDispatcherAggregationFunctions.cu:49-168). */
+int32_t qdb_gb_batch_result(qdb_gb_batch* b, int32_t inst, const int64_t** keys, const void** cols,
+                            int32_t* n_cols, int64_t* col_stride);
+/* Copies the result region of queries [first, first + n) to host memory: for each query, max_groups + 2 rows of
+ * (1 + n_cols) int64-sized words in the layout of qdb_gb_batch_result (keys first, then each column).
+ * host_bytes is the size of `host`; the needed size is returned in *needed (call with host == NULL to ask). */
+int32_t qdb_gb_batch_copy_results(qdb_gb_batch* b, int32_t first, int32_t n, void* host, int64_t host_bytes,
+                                  int64_t* needed, void* stream);
+/* Reads and overrides the plan of query `inst` (the override lasts until the next qdb_gb_batch_set). */
+int32_t qdb_gb_batch_get_cfg(qdb_gb_batch* b, int32_t inst, qdb_gb_batch_cfg* cfg);
+int32_t qdb_gb_batch_set_cfg(qdb_gb_batch* b, int32_t inst, const qdb_gb_batch_cfg* cfg);
+/* Times candidate plans on the batch's own queries (one run per candidate, every work item timed on the device)
+ * and records, per query class (value type, cardinality, rows), the plan with the lowest SM-time per row in the
+ * process-wide tuning table; then re-plans the batch from it.  Synchronises `stream`. */
+int32_t qdb_gb_batch_autotune(qdb_gb_batch* b, void* stream);
+/* Device time of the last run's aggregation kernel per work item, summed per query, in nanoseconds
+ * (host array of n entries; requires a run after qdb_gb_batch_autotune or with timing enabled). */
+int32_t qdb_gb_batch_item_times(qdb_gb_batch* b, int64_t* ns, void* stream);
+/* Clears the process-wide tuning table (plans fall back to the built-in heuristic). */
+int32_t qdb_gb_batch_tuning_reset(void);
+
 #ifdef __cplusplus
 }
 #endif

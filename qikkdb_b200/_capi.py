@@ -51,6 +51,33 @@ class qdb_pred(C.Structure):
     ]
 
 
+class qdb_gb_query(C.Structure):
+    _fields_ = [
+        ("agg_mask", C.c_int32),
+        ("key_type", C.c_int32),
+        ("val_type", C.c_int32),
+        ("reserved", C.c_int32),
+        ("keys", C.c_void_p),
+        ("vals", C.c_void_p),
+        ("n_rows", C.c_int64),
+        ("max_groups", C.c_int64),
+        ("key_mod", C.c_int64),
+        ("pred", qdb_pred),
+    ]
+
+
+class qdb_gb_batch_cfg(C.Structure):
+    _fields_ = [
+        ("placement", C.c_int32),
+        ("smem_slots", C.c_int32),
+        ("replicas", C.c_int32),
+        ("warps", C.c_int32),
+        ("rows_per_thread", C.c_int32),
+        ("reserved", C.c_int32),
+        ("chunk_rows", C.c_int64),
+    ]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 I32 = C.c_int32
@@ -90,6 +117,18 @@ SIGNATURES = [
     ("qdb_generate_indexes", I32, [P, I64, PP, PI64, P]),
     ("qdb_prefix_sum", I32, [P, I64, P, P]),
     ("qdb_compress_null_mask", I32, [P, I64, PP, P]),
+    ("qdb_gb_batch_create", I32, [PP, I32, I64, I64, P]),
+    ("qdb_gb_batch_destroy", I32, [P]),
+    ("qdb_gb_batch_set", I32, [P, C.POINTER(qdb_gb_query), I32, P]),
+    ("qdb_gb_batch_run", I32, [P, I32, P]),
+    ("qdb_gb_batch_fetch", I32, [P, PI64, C.POINTER(I32), P]),
+    ("qdb_gb_batch_result", I32, [P, I32, PP, PP, C.POINTER(I32), PI64]),
+    ("qdb_gb_batch_copy_results", I32, [P, I32, I32, P, I64, PI64, P]),
+    ("qdb_gb_batch_get_cfg", I32, [P, I32, C.POINTER(qdb_gb_batch_cfg)]),
+    ("qdb_gb_batch_set_cfg", I32, [P, I32, C.POINTER(qdb_gb_batch_cfg)]),
+    ("qdb_gb_batch_autotune", I32, [P, P]),
+    ("qdb_gb_batch_item_times", I32, [P, PI64, P]),
+    ("qdb_gb_batch_tuning_reset", I32, []),
 ]
 
 _lib = None

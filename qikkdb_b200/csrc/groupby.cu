@@ -13,7 +13,7 @@ namespace qdb {
 // ---------------------------------------------------------------------------------------------
 // Layout and sizing.
 // ---------------------------------------------------------------------------------------------
-static Layout make_layout(int32_t aggs, ValKind vk) {
+Layout make_layout(int32_t aggs, ValKind vk) {
     Layout L;
     const bool has_vals = vk != VK_NONE;
     int w = 1;
@@ -201,7 +201,7 @@ static PredInterval interval_t(const qdb_pred& p) {
     }
 }
 
-static PredInterval pred_interval(const qdb_pred& p) {
+PredInterval pred_interval(const qdb_pred& p) {
     switch (p.type) {
         case QDB_INT32: return interval_t<int32_t>(p);
         case QDB_INT64: return interval_t<int64_t>(p);

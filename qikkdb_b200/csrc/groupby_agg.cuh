@@ -848,6 +848,11 @@ int32_t launch_agg_k(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, si
     }
 }
 
+// Slot layout of a table carrying `aggs` over values of kind vk (groupby.cu).
+Layout make_layout(int32_t aggs, ValKind vk);
+// `col OP constant` as an interval of the column type (groupby.cu).
+PredInterval pred_interval(const qdb_pred& p);
+
 // Per-key-type entry points, each instantiated in its own translation unit.
 int32_t launch_agg_i32(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
 int32_t launch_agg_i64(const AggArgs& a, ValKind vk, int32_t ptype, bool nulls, size_t smem, cudaStream_t st);
