@@ -37,6 +37,12 @@ N_DISTINCT = 1_000_000
 BYTES_PER_ROW = 16  # 4 (predicate) + 8 (key) + 4 (value)
 SEED = 20240601
 METRIC = "filtered GROUP BY rows/s"
+BATCH_INSTANCES = 4096
+BATCH_SEED = 20240602
+BATCH_METRIC = "batched GROUP BY queries/s"
+BATCH_WORKLOAD = ("batched-4096: 4096 independent GROUP BY instances, rows log-uniform in [1K, 4M], cardinality "
+                  "log-uniform in [4, 64K], int32 keys uniform over the cardinality, int64 or f32 values (50/50), "
+                  "aggregates SUM+MIN+MAX+COUNT | SUM+AVG | SUM+COUNT+MAX")
 WORKLOAD = "filtered-groupby-256M: f32 pred p<0.5, int64 Zipf(1.1) keys over 1M, f32 lognormal(2,1) values, SUM+AVG"
 
 
@@ -49,6 +55,10 @@ def parse_args():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--cpu-sample-rows", type=int, default=1 << 25)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served"])
+    ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
+    ap.add_argument("--plain-sample", type=int, default=0,
+                    help="batched: queries of the one-by-one plain-path comparison (0 = all)")
     return ap.parse_args()
 
 
@@ -303,8 +313,258 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------------------------------------------
+# Batched workload: many independent GROUP BY queries in one persistent launch (CUDA graph) against the same
+# queries issued one by one through the plain path.
+# ---------------------------------------------------------------------------------------------------------------
+AGG_SHAPES = (("sum", "min", "max", "count"), ("sum", "avg"), ("sum", "count", "max"))
+
+
+def batched_instances(n_inst: int):
+    """Per-instance shape: (rows, cardinality, value dtype, aggregates); seeded."""
+    from qikkdb_b200 import datagen as dg
+    rows = dg.loguniform_i64(BATCH_SEED, 0, n_inst, 1000, 4_000_000)
+    card = dg.loguniform_i64(BATCH_SEED, 1, n_inst, 4, 65536)
+    pick = dg.uniform_i32(BATCH_SEED, 2, n_inst, 0, 5)
+    out = []
+    for i in range(n_inst):
+        vdt = np.int64 if pick[i] % 2 == 0 else np.float32
+        out.append((int(rows[i]), int(card[i]), vdt, AGG_SHAPES[int(pick[i]) // 2]))
+    return out
+
+
+def batched_columns(shapes, dev, host: bool = False):
+    """Keys and values of every instance (seeded per instance), 16-byte aligned slices of three device buffers."""
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    pad = lambda n: (n + 3) // 4 * 4  # noqa: E731
+    tot_k = sum(pad(r) for r, _, _, _ in shapes)
+    tot_i64 = sum(pad(r) for r, _, v, _ in shapes if v == np.int64)
+    tot_f32 = sum(pad(r) for r, _, v, _ in shapes if v == np.float32)
+    keys = torch.empty(tot_k, dtype=torch.int32, device=dev)
+    vi = torch.empty(max(tot_i64, 4), dtype=torch.int64, device=dev)
+    vf = torch.empty(max(tot_f32, 4), dtype=torch.float32, device=dev)
+    stage_k = torch.empty(4_000_004, dtype=torch.int32, pin_memory=True)
+    stage_v = torch.empty(4_000_004, dtype=torch.int64, pin_memory=True)
+    views, ok, oi, of = [], 0, 0, 0
+    hosts = []
+    for i, (r, c, vdt, _) in enumerate(shapes):
+        kh = stage_k.numpy()[:r]
+        dg.uniform_i32(BATCH_SEED + 1, i, r, 0, c - 1, out=kh)
+        kd = keys[ok:ok + r]
+        kd.copy_(stage_k[:r])
+        ok += pad(r)
+        if vdt == np.int64:
+            vh = stage_v.numpy()[:r]
+            dg.uniform_i64(BATCH_SEED + 2, i, r, -(1 << 40), 1 << 40, out=vh)
+            vd = vi[oi:oi + r]
+            vd.copy_(stage_v[:r])
+            oi += pad(r)
+        else:
+            vh = stage_v.numpy().view(np.float32)[:r]
+            dg.lognormal_f32(BATCH_SEED + 2, i, r, 2.0, 1.0, out=vh)
+            vd = vf[of:of + r]
+            vd.copy_(stage_v.view(torch.float32)[:r])
+            of += pad(r)
+        if host:
+            hosts.append((kh.copy(), vh.copy()))
+        views.append((kd, vd))
+        torch.cuda.synchronize(dev)
+    return views, hosts, (keys, vi, vf)
+
+
+def run_batched(args):
+    import ctypes as C
+
+    import torch
+
+    from qikkdb_b200 import _capi
+    from qikkdb_b200.batch import GroupByBatch, Query
+    from qikkdb_b200.groupby import AGG_CODES
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    shapes = batched_instances(args.instances)
+    views, _, bufs = batched_columns(shapes, dev)
+    rows_total = sum(r for r, _, _, _ in shapes)
+    bytes_total = sum(r * (4 + (8 if v == np.int64 else 4)) for r, _, v, _ in shapes)
+    queries = [Query(k, v, list(a), c) for (k, v), (r, c, _, a) in zip(views, shapes)]
+    table_bytes = sum(((1 << max(4, int(np.ceil(np.log2(c * 3 // 2 + 1))))) + 2) * 8 * 8 + 256 for _, c, _, _ in shapes)
+    result_bytes = sum((c + 2) * (1 + len(a)) * 8 for _, c, _, a in shapes)
+    b = GroupByBatch(len(queries), table_bytes, result_bytes)
+    st = torch.cuda.Stream(dev)
+    t0 = time.perf_counter()
+    b.set(queries, stream=st.cuda_stream)
+    torch.cuda.synchronize(dev)
+    set_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    b.autotune(stream=st.cuda_stream)
+    tune_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        b.run(graph=True, stream=st.cuda_stream)
+    counts, status = b.fetch(stream=st.cuda_stream)
+    assert (status == 0).all(), "batched run reported an error status"
+    launches0 = lib.qdb_launch_count()
+    sampler = ClockSampler(local)
+    ev = []
+    with sampler:
+        for _ in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            b.run(graph=True, stream=st.cuda_stream)
+            e1.record(st)
+            ev.append((e0, e1))
+        torch.cuda.synchronize(dev)
+    launches = lib.qdb_launch_count() - launches0
+    step_ms = [a.elapsed_time(z) for a, z in ev]
+    ms = statistics.median(step_ms)
+    value = len(queries) / (ms / 1e3)
+    groups = int(counts.sum())
+
+    # end to end through the C ABI: run + per-query counts/status + every result copied to host
+    need = C.c_int64()
+    _capi.check(lib.qdb_gb_batch_copy_results(b.handle, 0, len(queries), None, 0, C.byref(need), st.cuda_stream))
+    host_res = torch.empty(max(need.value, 8), dtype=torch.uint8, pin_memory=True)
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        b.run(graph=True, stream=st.cuda_stream)
+        b.fetch(stream=st.cuda_stream)
+        _capi.check(lib.qdb_gb_batch_copy_results(b.handle, 0, len(queries), host_res.data_ptr(), need.value,
+                                                  C.byref(need), st.cuda_stream))
+        if i >= args.warmup:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    em = statistics.median(e2e_ms)
+
+    # the same queries one by one through the plain path (create, ProcessBlock + Swap, GetResults, free)
+    sample = list(range(len(queries))) if args.plain_sample <= 0 else list(range(min(args.plain_sample, len(queries))))
+    outs = (C.c_void_p * 8)()
+    onulls = (C.c_void_p * 8)()
+    okeys = (C.c_void_p * 1)()
+    oknull = (C.c_void_p * 1)()
+    cnt = C.c_int64()
+    plain_groups = 0
+
+    def plain_pass():
+        nonlocal plain_groups
+        plain_groups = 0
+        for i in sample:
+            r, c, vdt, aggs = shapes[i]
+            kd, vd = views[i]
+            mask = 0
+            for a in aggs:
+                mask |= AGG_CODES[a]
+            h = C.c_void_p()
+            vt = _capi.QDB_INT64 if vdt == np.int64 else _capi.QDB_FLOAT
+            _capi.check(lib.qdb_gb_create(C.byref(h), mask, _capi.QDB_INT32, 1, vt, c, 0, st.cuda_stream))
+            kc = (C.c_void_p * 1)(kd.data_ptr())
+            _capi.check(lib.qdb_gb_process_sync(h, kc, None, vd.data_ptr(), None, r, None, None, st.cuda_stream))
+            codes = (C.c_int32 * len(aggs))(*[AGG_CODES[a] for a in aggs])
+            _capi.check(lib.qdb_gb_results_multi(h, len(aggs), codes, okeys, oknull, outs, onulls, C.byref(cnt),
+                                                 st.cuda_stream))
+            plain_groups += cnt.value
+            lib.qdb_free(okeys[0], st.cuda_stream)
+            for j in range(len(aggs)):
+                lib.qdb_free(outs[j], st.cuda_stream)
+            lib.qdb_gb_destroy(h)
+        torch.cuda.synchronize(dev)
+
+    plain_pass()  # warm-up (pool allocations, module load)
+    t0 = time.perf_counter()
+    plain_pass()
+    plain_s = time.perf_counter() - t0
+    plain_qps = len(sample) / plain_s
+    if not args.plain_sample:
+        assert plain_groups == groups, f"plain path groups {plain_groups} != batched {groups}"
+
+    peak, peak_kind = measured_peak()
+    achieved = bytes_total / (ms / 1e3) / 1e9
+    cpu = batched_cpu_baseline(shapes, args) if rank == 0 and world == 1 else None
+    line = {"metric": BATCH_METRIC, "value": value, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas only",
+            "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "instances": len(queries), "rows_total": rows_total,
+                       "bytes_total": bytes_total, "groups_total": groups, "l2": f"inputs ({bytes_total / 1e9:.1f} GB) > L2, no flush",
+                       "step": "one CUDA graph: table init (skipped after the first run) + persistent aggregation "
+                               "kernel + result kernel, all instances"},
+            "plain_one_by_one": {"value": plain_qps, "unit": "queries/s", "queries": len(sample),
+                                 "seconds": plain_s, "groups": plain_groups,
+                                 "path": "per query: qdb_gb_create, qdb_gb_process_sync, qdb_gb_results_multi, "
+                                         "qdb_free, qdb_gb_destroy (ctypes, wall clock)"},
+            "speedup_vs_plain": value / plain_qps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "whole graph (init + gb_batch_agg_kernel + results)",
+                         "algorithmic_bytes_per_launch": bytes_total, "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": len(queries) / (em / 1e3), "unit": "queries/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(need.value + len(queries) * 12), "ms_per_step": em,
+                    "path": "qdb_gb_batch_run (graph) + qdb_gb_batch_fetch + qdb_gb_batch_copy_results to pinned host; "
+                            "inputs device-resident"},
+            "set_ms": set_ms, "autotune_s": tune_s, "clocks": sampler.summary(), "gpu_launches": int(launches),
+            "step_ms_min_max": [min(step_ms), max(step_ms)]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def batched_cpu_baseline(shapes, args, budget_s: float = 15.0) -> dict:
+    """The oracle (hash-map GROUP BY, all host threads) on instances in workload order until budget_s."""
+    import oracle
+    from qikkdb_b200 import datagen as dg
+    done, secs, rows = 0, 0.0, 0
+    threads = 0
+    for i, (r, c, vdt, _) in enumerate(shapes):
+        k = dg.uniform_i32(BATCH_SEED + 1, i, r, 0, c - 1)
+        v = (dg.uniform_i64(BATCH_SEED + 2, i, r, -(1 << 40), 1 << 40) if vdt == np.int64
+             else dg.lognormal_f32(BATCH_SEED + 2, i, r, 2.0, 1.0))
+        res = oracle.groupby(k, v, threads=0, sort=False, timing_only=True)
+        secs += res["seconds"]
+        threads = res["threads"]
+        done += 1
+        rows += r
+        if secs >= budget_s:
+            break
+    return {"value": done / secs, "unit": "queries/s", "cores": threads, "kind": "port",
+            "sample": f"first {done} of {len(shapes)} instances ({rows} rows), hash-map GROUP BY per query, "
+                      f"{threads} threads, {secs:.2f} s"}
+
+
+def run_batched_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    shapes = batched_instances(args.instances)
+    secs = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = batched_cpu_baseline(shapes, args, budget_s=max(2.0, 20.0 / (args.warmup + args.steps)))
+        if i >= args.warmup:
+            secs.append(cb["value"])
+    value = statistics.mean(secs)
+    line = {"impl": "reference", "metric": BATCH_METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "replicas only", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "instances": len(shapes)},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cb["cores"], "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload == "batched":
+        if args.impl == "reference":
+            run_batched_reference(args)
+        else:
+            run_batched(args)
+        return
+    if args.workload == "served":
+        from bench_served import run_served  # noqa: F401  (defined below when the served workload is built)
     if args.impl == "reference":
         run_reference(args)
     else:
