@@ -380,7 +380,7 @@ def run_batched(args):
     import torch
 
     from qikkdb_b200 import _capi
-    from qikkdb_b200.batch import GroupByBatch, Query
+    from qikkdb_b200.batch import GroupByBatch, Query, required_bytes
     from qikkdb_b200.groupby import AGG_CODES
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -394,8 +394,7 @@ def run_batched(args):
     rows_total = sum(r for r, _, _, _ in shapes)
     bytes_total = sum(r * (4 + (8 if v == np.int64 else 4)) for r, _, v, _ in shapes)
     queries = [Query(k, v, list(a), c) for (k, v), (r, c, _, a) in zip(views, shapes)]
-    table_bytes = sum(((1 << max(4, int(np.ceil(np.log2(c * 3 // 2 + 1))))) + 2) * 8 * 8 + 256 for _, c, _, _ in shapes)
-    result_bytes = sum((c + 2) * (1 + len(a)) * 8 for _, c, _, a in shapes)
+    table_bytes, result_bytes = required_bytes(queries)
     b = GroupByBatch(len(queries), table_bytes, result_bytes)
     st = torch.cuda.Stream(dev)
     t0 = time.perf_counter()

@@ -258,8 +258,10 @@ typedef struct qdb_gb_batch_cfg {
                                 every work item; QDB_PLACE_GLOBAL: every row goes to the global table */
     int32_t smem_slots;      /* slots of one shared-memory table (a power of two >= 64), shared placement */
     int32_t replicas;        /* shared-memory tables per warp group (warp w uses table w % replicas) */
-    int32_t warps;           /* warps cooperating on one work item: 16, 8 or 4 (1, 2 or 4 groups per CTA) */
-    int32_t rows_per_thread; /* rows each thread loads per step: 4 or 8 */
+    int32_t warps;           /* consumer warps cooperating on one work item: 12, 6 or 3 (1, 2 or 4 warp groups per
+                                CTA, each with its own producer warp and share of shared memory) */
+    int32_t rows_per_thread; /* rows each consumer thread takes per step through a staged column tile: 1, 2 or 4
+                                (the probe loads of one step's rows are in flight together) */
     int32_t reserved;
     int64_t chunk_rows;      /* rows per work item (a multiple of 64) */
 } qdb_gb_batch_cfg;
@@ -304,6 +306,14 @@ int32_t qdb_gb_batch_autotune(qdb_gb_batch* b, void* stream);
 /* Device time of the last run's aggregation kernel per work item, summed per query, in nanoseconds
  * (host array of n entries; requires a run after qdb_gb_batch_autotune or with timing enabled). */
 int32_t qdb_gb_batch_item_times(qdb_gb_batch* b, int64_t* ns, void* stream);
+/* Device bytes that qdb_gb_batch_set needs for the tables and the results of these queries (for sizing a batch
+ * or admitting queries against a memory budget). */
+int32_t qdb_gb_batch_required(const qdb_gb_query* queries, int32_t n, int64_t* table_bytes, int64_t* result_bytes);
+/* share != 0 (the default): queries of the batch that read the same columns (same key, value and predicate
+ * columns and row count) and run with the same warp-group width are aggregated in one scan, up to 8 per scan,
+ * as long as their shared-memory tables fit one warp group together; each column tile is then loaded once for
+ * all of them.  share == 0: every query scans its columns on its own.  Re-plans the batch. */
+int32_t qdb_gb_batch_set_sharing(qdb_gb_batch* b, int32_t share);
 /* Clears the process-wide tuning table (plans fall back to the built-in heuristic). */
 int32_t qdb_gb_batch_tuning_reset(void);
 

@@ -128,6 +128,8 @@ SIGNATURES = [
     ("qdb_gb_batch_set_cfg", I32, [P, I32, C.POINTER(qdb_gb_batch_cfg)]),
     ("qdb_gb_batch_autotune", I32, [P, P]),
     ("qdb_gb_batch_item_times", I32, [P, PI64, P]),
+    ("qdb_gb_batch_required", I32, [C.POINTER(qdb_gb_query), I32, PI64, PI64]),
+    ("qdb_gb_batch_set_sharing", I32, [P, I32]),
     ("qdb_gb_batch_tuning_reset", I32, []),
 ]
 

@@ -168,6 +168,9 @@ class GroupByBatch:
             setattr(c, k, int(v))
         capi.check(capi.lib().qdb_gb_batch_set_cfg(self.handle, i, C.byref(c)))
 
+    def set_sharing(self, share: bool) -> None:
+        capi.check(capi.lib().qdb_gb_batch_set_sharing(self.handle, 1 if share else 0))
+
     def autotune(self, stream=None) -> None:
         capi.check(capi.lib().qdb_gb_batch_autotune(self.handle, _stream(stream)))
 
@@ -175,6 +178,14 @@ class GroupByBatch:
         ns = np.zeros(max(len(self.queries), 1), np.int64)
         capi.check(capi.lib().qdb_gb_batch_item_times(self.handle, ns.ctypes.data_as(capi.PI64), _stream(stream)))
         return ns[:len(self.queries)]
+
+
+def required_bytes(queries: Sequence[Query]) -> tuple:
+    """(table bytes, result bytes) that a batch of these queries needs (qdb_gb_batch_required)."""
+    arr = (capi.qdb_gb_query * max(len(queries), 1))(*[q.to_c() for q in queries])
+    t, r = C.c_int64(), C.c_int64()
+    capi.check(capi.lib().qdb_gb_batch_required(arr, len(queries), C.byref(t), C.byref(r)))
+    return t.value, r.value
 
 
 def tuning_reset() -> None:

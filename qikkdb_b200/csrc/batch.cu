@@ -5,6 +5,7 @@
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "batch.cuh"
@@ -18,9 +19,9 @@ __global__ void gb_batch_results_kernel(const BatchArgs ba);
 // A plan family the autotuner chooses between, independent of one query's sizes.
 struct BKind {
     int32_t place = QDB_PLACE_SHARED;  // QDB_PLACE_SHARED or QDB_PLACE_GLOBAL
-    int32_t rep = 0;                   // shared tables per group: 0 -> 1, 1 -> 4, 2 -> one per warp
-    int32_t warps = kBWarps;           // kBWarps, kBWarps / 2 or kBWarps / 4
-    int32_t ipt = 4;                   // 4 or 8
+    int32_t rep = 0;                   // shared tables per group: 0 -> 1, 1 -> 4, 2 -> one per consumer warp
+    int32_t warps = kBCons;            // consumer warps per group: kBCons, kBCons / 2 or kBCons / 4
+    int32_t rpt = 2;                   // rows each consumer thread takes from a stage tile (1..kBMaxRowsPerLane)
 };
 
 static uint64_t next_pow2_u(uint64_t x) {
@@ -35,7 +36,7 @@ static int ceil_log2(uint64_t x) {
     return l;
 }
 
-static int queue_of(int warps) { return warps == kBWarps ? 0 : (warps == kBWarps / 2 ? 1 : 2); }
+static int queue_of(int warps) { return warps == kBCons ? 0 : (warps == kBCons / 2 ? 1 : 2); }
 
 // Process-wide tuning table: query class -> best plan family.
 static std::mutex g_tune_mu;
@@ -49,6 +50,12 @@ static uint64_t class_key(const qdb_gb_query& q) {
     const uint64_t cb = static_cast<uint64_t>(ceil_log2(std::max<uint64_t>(card, 1)));
     const uint64_t rb = static_cast<uint64_t>(ceil_log2(static_cast<uint64_t>(std::max<int64_t>(q.n_rows, 1))) / 2);
     return vk | (kt << 3) | (pr << 4) | (cb << 5) | (rb << 11);
+}
+
+// Hashed slots of a query's global table: load factor at most 0.4, so that most probe sequences end at their first
+// slot (every further probe is a dependent L2 round trip).
+static uint64_t batch_table_cap(int64_t max_groups) {
+    return next_pow2_u(std::max<uint64_t>(16, static_cast<uint64_t>(max_groups) * 5 / 2 + 1));
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -76,6 +83,7 @@ struct qdb_gb_batch {
     qdb::BHeader* d_hdr = nullptr;
     qdb::BInst* d_inst = nullptr;
     qdb::BItem* d_items = nullptr;
+    qdb::BGroup* d_groups = nullptr;
     uint64_t* d_tables = nullptr;
     uint64_t* d_res = nullptr;
     unsigned long long* d_counters = nullptr;
@@ -86,12 +94,16 @@ struct qdb_gb_batch {
     qdb::BHeader* h_hdr = nullptr;
     qdb::BInst* h_inst = nullptr;
     qdb::BItem* h_items = nullptr;
+    qdb::BGroup* h_groups = nullptr;
     cudaEvent_t upload_done = nullptr;
     bool upload_recorded = false;
     // plan
     std::vector<qdb_gb_query> q;
     std::vector<qdb_gb_batch_cfg> cfg;
     std::vector<qdb::BItem> items;
+    std::vector<int32_t> inst_group;   // scan group of every query
+    int32_t n_groups = 0;
+    bool share = true;                 // queries over the same columns share one scan
     int32_t n = 0;
     bool dirty = false;
     bool needs_init = false;
@@ -114,6 +126,7 @@ static BatchArgs batch_args(const qdb_gb_batch* b) {
     a.hdr = b->d_hdr;
     a.inst = b->d_inst;
     a.items = b->d_items;
+    a.groups = b->d_groups;
     a.res = b->d_res;
     a.res_count = b->d_res_count;
     a.status = b->d_status;
@@ -122,28 +135,31 @@ static BatchArgs batch_args(const qdb_gb_batch* b) {
     return a;
 }
 
-// Shared-memory bytes of one warp group at a given width.
-static size_t group_bytes(const qdb_gb_batch* b, int warps) {
+// Shared-memory bytes available for the tables of one warp group at a given width.
+static size_t table_space(const qdb_gb_batch* b, int warps) {
     const int q = queue_of(warps);
-    return (b->dyn_bytes >> q) & ~static_cast<size_t>(127);
+    const size_t gbytes = (b->dyn_bytes >> q) & ~static_cast<size_t>(127);
+    return gbytes - kBHeaderBytes - b_ring_bytes(q);
 }
+
+static size_t align128(size_t x) { return (x + 127) & ~static_cast<size_t>(127); }
 
 // The plan of query i for a plan family: falls back to the global table when the shared tables do not fit.
 static qdb_gb_batch_cfg apply_kind(const qdb_gb_batch* b, const qdb_gb_query& q, const BKind& k) {
     qdb_gb_batch_cfg c{};
     c.warps = k.warps;
-    c.rows_per_thread = k.ipt;
+    c.rows_per_thread = k.rpt;
     c.placement = QDB_PLACE_GLOBAL;
     c.smem_slots = 0;
     c.replicas = 1;
     const int64_t card = std::min<int64_t>(q.max_groups + 1, std::max<int64_t>(q.n_rows, 1));
     if (k.place == QDB_PLACE_SHARED) {
         const size_t bps = smem_slot_bytes(q);
-        const size_t gb = group_bytes(b, k.warps);
+        const size_t gb = table_space(b, k.warps);
         const int S = static_cast<int>(next_pow2_u(static_cast<uint64_t>(std::max<int64_t>(64, 2 * card))));
         int R = (k.rep == 0) ? 1 : (k.rep == 1 ? std::min(4, k.warps) : k.warps);
-        while (R > 1 && static_cast<size_t>(R) * S * bps > gb) --R;
-        if (static_cast<size_t>(S) * bps <= gb && S <= (1 << 20)) {
+        while (R > 1 && align128(static_cast<size_t>(R) * S * bps) > gb) --R;
+        if (align128(static_cast<size_t>(S) * bps) <= gb && S <= (1 << 20)) {
             c.placement = QDB_PLACE_SHARED;
             c.smem_slots = S;
             c.replicas = R;
@@ -152,7 +168,7 @@ static qdb_gb_batch_cfg apply_kind(const qdb_gb_batch* b, const qdb_gb_query& q,
     // Work items: big queries are cut so that every SM gets several items; an item of a shared placement is
     // long enough to amortise clearing and merging its tables.
     const int64_t per_sm = std::max<int64_t>(b->total_rows / (static_cast<int64_t>(b->grid) * 8), 1);
-    int64_t chunk = std::min<int64_t>(std::max<int64_t>(per_sm * k.warps / kBWarps, 32768), int64_t(8) << 20);
+    int64_t chunk = std::min<int64_t>(std::max<int64_t>(per_sm * k.warps / kBCons, 32768), int64_t(8) << 20);
     if (c.placement == QDB_PLACE_SHARED)
         chunk = std::max<int64_t>(chunk, int64_t(16) * c.replicas * c.smem_slots);
     chunk = (chunk + 63) / 64 * 64;
@@ -165,8 +181,8 @@ static BKind heuristic_kind(const qdb_gb_query& q) {
     const int64_t card = std::min<int64_t>(q.max_groups + 1, std::max<int64_t>(q.n_rows, 1));
     k.place = QDB_PLACE_SHARED;
     k.rep = card <= 32 ? 2 : (card <= 512 ? 1 : 0);
-    k.warps = q.n_rows < 65536 ? kBWarps / 4 : (q.n_rows < 524288 ? kBWarps / 2 : kBWarps);
-    k.ipt = 4;
+    k.warps = q.n_rows < 65536 ? kBCons / 4 : (q.n_rows < 524288 ? kBCons / 2 : kBCons);
+    k.rpt = 2;
     return k;
 }
 
@@ -182,19 +198,93 @@ static int64_t result_words(const qdb_gb_query& q) {
     return rows * (1 + __builtin_popcount(static_cast<unsigned>(q.agg_mask)));
 }
 
-// Rebuilds the work items from the current plans and stages the descriptors for upload.
+// Rows of one stage tile of a group: as many as fit one ring stage (a multiple of 128 rows, so every column's
+// tile is a whole number of 16-byte units and the rows spread evenly over the group's lanes).
+static int stage_rows(int warps, int kt, int vb, int pb) {
+    const int q = queue_of(warps);
+    auto bytes = [&](int t) { return align128(size_t(t) * kt) + align128(size_t(t) * vb) + align128(size_t(t) * pb); };
+    int T = 128;
+    while (bytes(T + 128) <= static_cast<size_t>(b_stage_bytes(q))) T += 128;
+    return T;
+}
+
+// Bytes of one query's shared tables.
+static size_t query_table_bytes(const qdb_gb_query& q, const qdb_gb_batch_cfg& c) {
+    if (c.placement != QDB_PLACE_SHARED) return 0;
+    return align128(static_cast<size_t>(c.replicas) * c.smem_slots * smem_slot_bytes(q));
+}
+
+// Forms the scan groups (queries over the same columns, with the same warp-group width and tile, whose shared
+// tables fit one group together), cuts every group into work items and stages the descriptors for upload.
 static int32_t build_items(qdb_gb_batch* b) {
-    std::vector<BItem> its[kBQueues];
+    struct Key {
+        const void* k;
+        const void* v;
+        const void* p;
+        int64_t n;
+        int32_t kt, vt, pt, warps, rpt;
+        bool operator<(const Key& o) const {
+            return std::tie(k, v, p, n, kt, vt, pt, warps, rpt) < std::tie(o.k, o.v, o.p, o.n, o.kt, o.vt, o.pt, o.warps, o.rpt);
+        }
+    };
+    std::vector<std::vector<int>> members;
+    std::vector<size_t> used;
+    std::map<Key, std::vector<int>> open;  // key -> indices of groups that may take more members
+    b->inst_group.assign(b->n, -1);
     for (int i = 0; i < b->n; ++i) {
         const qdb_gb_query& q = b->q[i];
         const qdb_gb_batch_cfg& c = b->cfg[i];
+        const size_t tb = query_table_bytes(q, c);
+        const Key key{q.keys, q.val_type ? q.vals : nullptr, q.pred.col, q.n_rows, q.key_type, q.val_type,
+                      q.pred.col ? q.pred.type : 0, c.warps, c.rows_per_thread};
+        int gi = -1;
+        if (b->share && q.n_rows > 0) {
+            for (int cand : open[key])
+                if (members[cand].size() < static_cast<size_t>(kBMaxMembers) && used[cand] + tb <= table_space(b, c.warps)) {
+                    gi = cand;
+                    break;
+                }
+        }
+        if (gi < 0) {
+            gi = static_cast<int>(members.size());
+            members.emplace_back();
+            used.push_back(0);
+            open[key].push_back(gi);
+        }
+        b->h_inst[i].so_table = static_cast<int32_t>(used[gi]);
+        used[gi] += tb;
+        members[gi].push_back(i);
+        b->inst_group[i] = gi;
+    }
+    b->n_groups = static_cast<int32_t>(members.size());
+    std::vector<BItem> its[kBQueues];
+    for (int gi = 0; gi < b->n_groups; ++gi) {
+        const int i0 = members[gi][0];
+        const qdb_gb_query& q = b->q[i0];
+        const qdb_gb_batch_cfg& c = b->cfg[i0];
+        BGroup& G = b->h_groups[gi];
+        memset(&G, 0, sizeof(G));
+        G.keys = q.keys;
+        G.vals = q.val_type ? q.vals : nullptr;
+        G.pcol = q.pred.col;
+        G.n = q.n_rows;
+        G.kt = type_size(q.key_type);
+        G.vbytes = q.val_type ? type_size(q.val_type) : 0;
+        G.pbytes = q.pred.col ? type_size(q.pred.type) : 0;
+        G.vk = val_kind(q.val_type);
+        G.n_members = static_cast<int32_t>(members[gi].size());
+        for (int k = 0; k < G.n_members; ++k) G.members[k] = members[gi][k];
+        G.stage_rows = stage_rows(c.warps, G.kt, G.vbytes, G.pbytes);
+        G.rpt = c.rows_per_thread;
+        int64_t chunk = c.chunk_rows;
+        for (int m : members[gi]) chunk = std::min<int64_t>(chunk, b->cfg[m].chunk_rows);
         const int qi = queue_of(c.warps);
-        for (int64_t r = 0; r < q.n_rows; r += c.chunk_rows) {
+        for (int64_t r = 0; r < q.n_rows; r += chunk) {
             BItem it{};
-            it.inst = i;
+            it.group = gi;
             it.queue = qi;
             it.r0 = r;
-            it.r1 = std::min<int64_t>(q.n_rows, r + c.chunk_rows);
+            it.r1 = std::min<int64_t>(q.n_rows, r + chunk);
             its[qi].push_back(it);
         }
     }
@@ -210,7 +300,7 @@ static int32_t build_items(qdb_gb_batch* b) {
     if (static_cast<int64_t>(b->items.size()) > b->max_items) {
         // Grow the item buffers (the captured graph holds the old pointers).
         const int64_t want = static_cast<int64_t>(b->items.size()) * 2;
-        cudaEventSynchronize(b->upload_done);
+        if (b->upload_recorded) cudaEventSynchronize(b->upload_done);
         cudaDeviceSynchronize();
         cudaFree(b->d_items);
         cudaFree(b->d_item_ns);
@@ -231,7 +321,6 @@ static int32_t build_items(qdb_gb_batch* b) {
         I.S = c.placement == QDB_PLACE_SHARED ? c.smem_slots : 0;
         I.R = c.placement == QDB_PLACE_SHARED ? c.replicas : 1;
         I.probe = std::min(I.S, 32);
-        I.ipt = c.rows_per_thread;
     }
     b->h_hdr->n_inst = b->n;
     for (int qi = 0; qi < kBQueues; ++qi) b->h_hdr->heads[qi] = 0;
@@ -244,6 +333,8 @@ static int32_t upload(qdb_gb_batch* b, cudaStream_t s) {
     QDB_CUDA_TRY(cudaMemcpyAsync(b->d_hdr, b->h_hdr, sizeof(BHeader), cudaMemcpyHostToDevice, s));
     if (b->n > 0)
         QDB_CUDA_TRY(cudaMemcpyAsync(b->d_inst, b->h_inst, b->n * sizeof(BInst), cudaMemcpyHostToDevice, s));
+    if (b->n_groups > 0)
+        QDB_CUDA_TRY(cudaMemcpyAsync(b->d_groups, b->h_groups, b->n_groups * sizeof(BGroup), cudaMemcpyHostToDevice, s));
     if (!b->items.empty())
         QDB_CUDA_TRY(cudaMemcpyAsync(b->d_items, b->h_items, b->items.size() * sizeof(BItem),
                                      cudaMemcpyHostToDevice, s));
@@ -303,16 +394,16 @@ static int32_t check_query(const qdb_gb_query& q) {
 }
 
 static int32_t check_cfg(const qdb_gb_batch* b, const qdb_gb_query& q, const qdb_gb_batch_cfg& c) {
-    if (c.warps != kBWarps && c.warps != kBWarps / 2 && c.warps != kBWarps / 4)
-        return fail(QDB_ERR_INVALID, "batch cfg: warps must be 16, 8 or 4");
-    if (c.rows_per_thread != 4 && c.rows_per_thread != 8)
-        return fail(QDB_ERR_INVALID, "batch cfg: rows_per_thread must be 4 or 8");
+    if (c.warps != kBCons && c.warps != kBCons / 2 && c.warps != kBCons / 4)
+        return fail(QDB_ERR_INVALID, "batch cfg: warps must be 12, 6 or 3");
+    if (c.rows_per_thread != 1 && c.rows_per_thread != 2 && c.rows_per_thread != 4)
+        return fail(QDB_ERR_INVALID, "batch cfg: rows_per_thread must be 1, 2 or 4");
     if (c.chunk_rows < 64 || c.chunk_rows % 64) return fail(QDB_ERR_INVALID, "batch cfg: chunk_rows must be a positive multiple of 64");
     if (c.placement == QDB_PLACE_SHARED) {
         const int S = c.smem_slots;
         if (S < 64 || (S & (S - 1))) return fail(QDB_ERR_INVALID, "batch cfg: smem_slots must be a power of two >= 64");
         if (c.replicas < 1 || c.replicas > c.warps) return fail(QDB_ERR_INVALID, "batch cfg: replicas must be in [1, warps]");
-        if (static_cast<size_t>(c.replicas) * S * smem_slot_bytes(q) > group_bytes(b, c.warps))
+        if (query_table_bytes(q, c) > table_space(b, c.warps))
             return fail(QDB_ERR_TOO_LARGE, "batch cfg: shared-memory tables do not fit the warp group");
     } else if (c.placement != QDB_PLACE_GLOBAL) {
         return fail(QDB_ERR_INVALID, "batch cfg: placement must be SHARED or GLOBAL");
@@ -391,7 +482,8 @@ int32_t qdb_gb_batch_create(qdb_gb_batch** out, int32_t max_instances, int64_t t
     cudaFuncAttributes fa;
     try_cuda(cudaFuncGetAttributes(&fa, gb_batch_agg_kernel), "cudaFuncGetAttributes(gb_batch_agg_kernel)");
     if (rc == QDB_OK) {
-        b->dyn_bytes = (static_cast<size_t>(di.max_smem_optin) - fa.sharedSizeBytes - 256) & ~static_cast<size_t>(1023);
+        const size_t cap = std::min<size_t>(static_cast<size_t>(di.max_smem_optin), kBSmemCap);
+        b->dyn_bytes = (cap - fa.sharedSizeBytes - 256) & ~static_cast<size_t>(1023);
         try_cuda(cudaFuncSetAttribute(gb_batch_agg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(b->dyn_bytes)),
                  "cudaFuncSetAttribute(gb_batch_agg_kernel)");
@@ -399,6 +491,8 @@ int32_t qdb_gb_batch_create(qdb_gb_batch** out, int32_t max_instances, int64_t t
     try_cuda(cudaMalloc(&b->d_hdr, sizeof(BHeader)), "cudaMalloc(batch header)");
     try_cuda(cudaMalloc(&b->d_inst, max_instances * sizeof(BInst)), "cudaMalloc(batch descriptors)");
     try_cuda(cudaMalloc(&b->d_items, b->max_items * sizeof(BItem)), "cudaMalloc(batch items)");
+    try_cuda(cudaMalloc(&b->d_groups, max_instances * sizeof(BGroup)), "cudaMalloc(batch scan groups)");
+    try_cuda(cudaMallocHost(&b->h_groups, max_instances * sizeof(BGroup)), "cudaMallocHost(batch scan groups)");
     try_cuda(cudaMalloc(&b->d_item_ns, b->max_items * sizeof(long long)), "cudaMalloc(batch item times)");
     if (table_bytes > 0) try_cuda(cudaMalloc(&b->d_tables, table_bytes), "cudaMalloc(batch tables)");
     if (result_bytes > 0) try_cuda(cudaMalloc(&b->d_res, result_bytes), "cudaMalloc(batch results)");
@@ -437,6 +531,7 @@ int32_t qdb_gb_batch_destroy(qdb_gb_batch* b) {
     cudaFree(b->d_inst);
     cudaFree(b->d_items);
     cudaFree(b->d_item_ns);
+    cudaFree(b->d_groups);
     cudaFree(b->d_tables);
     cudaFree(b->d_res);
     cudaFree(b->d_counters);
@@ -445,6 +540,7 @@ int32_t qdb_gb_batch_destroy(qdb_gb_batch* b) {
     if (b->h_hdr) cudaFreeHost(b->h_hdr);
     if (b->h_inst) cudaFreeHost(b->h_inst);
     if (b->h_items) cudaFreeHost(b->h_items);
+    if (b->h_groups) cudaFreeHost(b->h_groups);
     if (b->upload_done) cudaEventDestroy(b->upload_done);
     if (prev != b->device) cudaSetDevice(prev);
     delete b;
@@ -461,7 +557,7 @@ int32_t qdb_gb_batch_set(qdb_gb_batch* b, const qdb_gb_query* queries, int32_t n
         int32_t rc = check_query(qs[i]);
         if (rc != QDB_OK) return rc;
         if (qs[i].max_groups > (int64_t(1) << 30)) qs[i].max_groups = int64_t(1) << 30;
-        const uint64_t cap = next_pow2_u(std::max<uint64_t>(16, static_cast<uint64_t>(qs[i].max_groups) * 3 / 2 + 1));
+        const uint64_t cap = batch_table_cap(qs[i].max_groups);
         const Layout L = make_layout(qs[i].agg_mask, val_kind(qs[i].val_type));
         toff[i] = table_off;
         table_off += static_cast<int64_t>((cap + 2) * L.W * 8 + 255) / 256 * 256;
@@ -483,10 +579,7 @@ int32_t qdb_gb_batch_set(qdb_gb_batch* b, const qdb_gb_query* queries, int32_t n
         BInst& I = b->h_inst[i];
         memset(&I, 0, sizeof(I));
         const ValKind vk = val_kind(q.val_type);
-        const uint64_t cap = next_pow2_u(std::max<uint64_t>(16, static_cast<uint64_t>(q.max_groups) * 3 / 2 + 1));
-        I.keys = q.keys;
-        I.vals = q.val_type ? q.vals : nullptr;
-        I.pcol = q.pred.col;
+        const uint64_t cap = batch_table_cap(q.max_groups);
         I.counters = b->d_counters + 2 * i;
         I.main.slots = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(b->d_tables) + toff[i]);
         I.main.mask = cap - 1;
@@ -589,7 +682,10 @@ int32_t qdb_gb_batch_item_times(qdb_gb_batch* b, int64_t* ns, void* stream) {
         QDB_CUDA_TRY(cudaMemcpyAsync(t.data(), b->d_item_ns, t.size() * sizeof(long long), cudaMemcpyDeviceToHost, s));
     QDB_CUDA_TRY(cudaStreamSynchronize(s));
     for (int i = 0; i < b->n; ++i) ns[i] = 0;
-    for (size_t k = 0; k < t.size(); ++k) ns[b->items[k].inst] += t[k];
+    for (size_t k = 0; k < t.size(); ++k) {
+        const BGroup& G = b->h_groups[b->items[k].group];
+        for (int m = 0; m < G.n_members; ++m) ns[G.members[m]] += t[k] / G.n_members;
+    }
     return QDB_OK;
 }
 
@@ -618,7 +714,7 @@ int32_t qdb_gb_batch_autotune(qdb_gb_batch* b, void* stream) {
         if (rc == QDB_OK) rc = qdb_gb_batch_item_times(b, ns.data(), stream);
         if (rc != QDB_OK) return rc;
         cost.assign(n, 0.0);
-        for (int i = 0; i < n; ++i) cost[i] = static_cast<double>(ns[i]) * b->cfg[i].warps / kBWarps;
+        for (int i = 0; i < n; ++i) cost[i] = static_cast<double>(ns[i]) * b->cfg[i].warps / kBCons;
         return QDB_OK;
     };
     // Coordinate search: placement and replication, then warp-group width, then rows per thread.
@@ -636,15 +732,15 @@ int32_t qdb_gb_batch_autotune(qdb_gb_batch* b, void* stream) {
                 cands.push_back(ks);
             }
         } else if (stage == 1) {
-            for (int w : {kBWarps, kBWarps / 2, kBWarps / 4}) {
+            for (int w : {kBCons, kBCons / 2, kBCons / 4}) {
                 std::vector<BKind> ks(best);
                 for (BKind& k : ks) k.warps = w;
                 cands.push_back(ks);
             }
         } else {
-            for (int ipt : {4, 8}) {
+            for (int rpt : {1, 2, 4}) {
                 std::vector<BKind> ks(best);
-                for (BKind& k : ks) k.ipt = ipt;
+                for (BKind& k : ks) k.rpt = rpt;
                 cands.push_back(ks);
             }
         }
@@ -675,6 +771,30 @@ int32_t qdb_gb_batch_autotune(qdb_gb_batch* b, void* stream) {
     rc = build_items(b);
     if (rc != QDB_OK) return rc;
     return upload(b, s);
+}
+
+int32_t qdb_gb_batch_required(const qdb_gb_query* queries, int32_t n, int64_t* table_bytes, int64_t* result_bytes) {
+    if (n < 0 || (n > 0 && !queries)) return fail(QDB_ERR_INVALID, "qdb_gb_batch_required: bad query list");
+    int64_t t = 0, r = 0;
+    for (int i = 0; i < n; ++i) {
+        qdb_gb_query q = queries[i];
+        if (q.max_groups < 1) return fail(QDB_ERR_INVALID, "qdb_gb_batch_required: max_groups must be >= 1");
+        if (q.max_groups > (int64_t(1) << 30)) q.max_groups = int64_t(1) << 30;
+        const Layout L = make_layout(q.agg_mask, val_kind(q.val_type));
+        t += static_cast<int64_t>((batch_table_cap(q.max_groups) + 2) * L.W * 8 + 255) / 256 * 256;
+        r += result_words(q) * 8;
+    }
+    if (table_bytes) *table_bytes = t;
+    if (result_bytes) *result_bytes = r;
+    return QDB_OK;
+}
+
+int32_t qdb_gb_batch_set_sharing(qdb_gb_batch* b, int32_t share) {
+    if (!b) return fail(QDB_ERR_INVALID, "qdb_gb_batch_set_sharing: null batch");
+    int32_t rc = wait_staging(b);
+    if (rc != QDB_OK) return rc;
+    b->share = share != 0;
+    return build_items(b);
 }
 
 int32_t qdb_gb_batch_tuning_reset(void) {

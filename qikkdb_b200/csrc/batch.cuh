@@ -5,18 +5,26 @@
 
 namespace qdb {
 
-constexpr int kBWarps = 16;                  // warps per CTA of the batch kernel
-constexpr int kBThreads = kBWarps * 32;      // 512 threads: 128 registers per thread at one CTA per SM, no spills
-constexpr int kBQueues = 3;                  // work queues for 1, 2 and 4 warp groups per CTA (16, 8, 4 warps)
+constexpr int kBCons = 12;                          // consumer warps per CTA
+constexpr int kBProd = 4;                           // producer warps per CTA (one per warp group)
+constexpr int kBThreads = (kBCons + kBProd) * 32;   // 512 threads (128 registers each), one CTA per SM
+constexpr int kBQueues = 3;                         // work queues for 1, 2 and 4 warp groups per CTA (12, 6, 3 warps)
+constexpr int kBStages = 3;                         // shared-memory ring stages per warp group
+constexpr int kBStageBytes = 24 * 1024;             // stage bytes at one group per CTA (halved per extra group level)
+constexpr int kBHeaderBytes = 256;                  // mbarriers and stage metadata of one warp group
+constexpr int kBMaxMembers = 8;                     // queries sharing one scan of their columns
+constexpr int kBMaxRowsPerLane = 4;
+constexpr int kBSmemCap = 192 * 1024;              // shared memory per CTA: the rest stays L1 for the probe loads
 constexpr int kBResThreads = 256;
 constexpr int kBResPer = 16;
 constexpr int kBResChunk = kBResThreads * kBResPer;
 
-// One query of the batch as the kernels see it (copied into shared memory at the start of every work item).
+// Shared memory of one warp group in queue q: [header | tables ... | stage ring].
+__host__ __device__ constexpr int b_stage_bytes(int q) { return kBStageBytes >> q; }
+__host__ __device__ constexpr int b_ring_bytes(int q) { return kBStages * (kBStageBytes >> q); }
+
+// One query of the batch as the kernels see it.
 struct BInst {
-    const void* keys;
-    const void* vals;
-    const void* pcol;
     unsigned long long* counters;  // [0] groups claimed, [1] status word
     Region main;                   // the query's global table (cap hashed slots + NULL slot + escape slot)
     int64_t n;
@@ -34,16 +42,30 @@ struct BInst {
     int32_t has_sum, has_min, has_max;
     int32_t aggs;
     int32_t S;                     // slots of one shared-memory table (power of two), 0 = global placement
-    int32_t R;                     // shared-memory tables per warp group
+    int32_t R;                     // shared-memory tables of this query per warp group
     int32_t probe;                 // shared-memory probe limit
-    int32_t ipt;                   // rows per thread per step (4 or 8)
+    int32_t so_table;              // byte offset of this query's shared tables in the group's table region
     int32_t pad;
 };
-static_assert(sizeof(BInst) % 8 == 0, "BInst is copied as 64-bit words");
+static_assert(sizeof(BInst) % 8 == 0, "BInst is 64-bit aligned");
 
-// A contiguous row range of one query.
+// Queries that read the same columns and are aggregated in one scan (one tile load serves every member).
+struct BGroup {
+    const void* keys;
+    const void* vals;
+    const void* pcol;
+    int64_t n;
+    int32_t kt, vbytes, pbytes, vk;
+    int32_t n_members;
+    int32_t stage_rows;            // rows per stage tile (as many as fit one ring stage, a multiple of 4)
+    int32_t rpt;                   // rows each consumer thread handles per step of a tile (1, 2 or 4)
+    int32_t pad;
+    int32_t members[kBMaxMembers];
+};
+
+// A contiguous row range of one scan group.
 struct BItem {
-    int32_t inst;
+    int32_t group;
     int32_t queue;
     int64_t r0;
     int64_t r1;
@@ -57,11 +79,14 @@ struct BHeader {
     int32_t q_begin[kBQueues + 1];  // queue q holds items [q_begin[q], q_begin[q + 1])
     int32_t n_inst;
     int32_t init_needed;
+    int32_t error;                  // QDB_ERR_TIMEOUT when a bounded wait gave up (reset by the init kernel)
+    int32_t pad;
 };
 
 struct BatchArgs {
     BHeader* hdr;
     const BInst* inst;
+    const BGroup* groups;
     const BItem* items;
     uint64_t* res;        // result words
     int64_t* res_count;   // per query: groups emitted

@@ -3,28 +3,29 @@
 // :395-410) and one GetResults per query (:478-587); here every query of a batch is a set of work items in
 // one launch.
 //
-// Aggregation kernel: one CTA of 16 warps per SM.  The CTA drains three work queues in turn; in queue q the
-// CTA is split into 2^q warp groups (16, 8 or 4 warps) that take work items independently, each with its
-// own share of shared memory and its own named barrier, so small queries do not hold a whole SM.  A work
-// item is a row range of one query.  The group streams the rows with 128-bit evict-first loads (each thread
-// 4 or 8 consecutive rows per step), evaluates the WHERE interval, applies the key modulus and inserts the
-// row
-//   * shared placement: into one of R shared-memory tables of the group (warp w uses table w % R, so
-//     low-cardinality queries spread their same-key atomics over R copies), then at the end of the item
-//     every occupied shared slot is merged into the query's global table;
-//   * global placement: straight into the query's global table, the probe loads of a thread's rows issued
-//     together.
+// Aggregation kernel: one CTA per SM of 12 consumer warps and 4 producer warps.  The CTA drains three work queues
+// in turn; in queue q it is split into 2^q warp groups (12, 6 or 3 consumer warps plus one producer warp), each
+// with its own share of shared memory, so that small queries do not hold a whole SM.  A work item is a row range
+// of a scan group: up to kBMaxMembers queries over the same columns.  Per group:
+//   * the producer warp takes items from the queue and streams their column tiles (keys, values, predicate
+//     column) into a ring of shared-memory stages with bulk asynchronous copies (cp.async.bulk, TMA engine)
+//     completing on per-stage mbarriers; the copies of the next item overlap the merge of the current one;
+//   * the consumer warps take the stages in order and apply every member query to the tile: WHERE interval,
+//     key modulus, then the insert
+//       - shared placement: into one of the query's R shared-memory tables (warp w uses table w % R, so
+//         low-cardinality queries spread their same-key atomics over R copies); after the item's last tile every
+//         occupied shared slot is merged into the query's global table;
+//       - global placement: straight into the query's global table, each lane issuing the probe loads of all
+//         its rows of the tile before completing any of them.
 // Rows whose shared-memory probe fails (a cardinality estimate that was too low) go to the global table.
-// Every item is timed with the global timer for the autotuner.
+// All waits (ring stages, consumer-group syncs) are mbarrier waits with an iteration limit; a wait that gives up
+// records QDB_ERR_TIMEOUT, which the result kernel reports for every query.  Every item is timed with the global
+// timer for the autotuner.
 #include <climits>
 
 #include "batch.cuh"
 
 namespace qdb {
-
-__device__ __forceinline__ void group_sync(int id, int nthreads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
-}
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -32,10 +33,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait on phase `parity`; gives up after kMaxWaitIters tries and records QDB_ERR_TIMEOUT in *err.
+__device__ __forceinline__ bool b_wait(uint64_t* bar, uint32_t parity, int32_t* err) {
+    for (uint32_t it = 0; it < kMaxWaitIters; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (it >= 16) __nanosleep(64);
+    }
+    atomicExch(err, static_cast<int>(QDB_ERR_TIMEOUT));
+    return false;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Table initialisation (only after a new plan: the result kernel cleans every slot it reads).
 // ---------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) gb_batch_init_kernel(const BatchArgs ba) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ba.hdr->error = 0;
     if (!ba.hdr->init_needed) return;
     const int i = blockIdx.x;
     if (i >= ba.hdr->n_inst) return;
@@ -54,59 +70,6 @@ __global__ void __launch_bounds__(1024) gb_batch_init_kernel(const BatchArgs ba)
     if (threadIdx.x == 0) {
         I.counters[0] = 0;
         I.counters[1] = 0;
-    }
-}
-
-// ---------------------------------------------------------------------------------------------
-// Row loads.  base is a multiple of IPT and the columns are 16-byte aligned, so a full step is IPT * size / 16
-// vector loads.
-// ---------------------------------------------------------------------------------------------
-template <int IPT>
-__device__ __forceinline__ void load_i32(const void* col, int64_t base, bool full, int64_t r1, int32_t (&out)[IPT]) {
-    const int32_t* p = static_cast<const int32_t*>(col) + base;
-    if (full) {
-#pragma unroll
-        for (int j = 0; j < IPT / 4; ++j) {
-            const int4 q = ld_stream16(p + 4 * j);
-            out[4 * j + 0] = q.x;
-            out[4 * j + 1] = q.y;
-            out[4 * j + 2] = q.z;
-            out[4 * j + 3] = q.w;
-        }
-    } else {
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) out[e] = (base + e < r1) ? p[e] : 0;
-    }
-}
-
-template <int IPT>
-__device__ __forceinline__ void load_i64(const void* col, int64_t base, bool full, int64_t r1, int64_t (&out)[IPT]) {
-    const int64_t* p = static_cast<const int64_t*>(col) + base;
-    if (full) {
-#pragma unroll
-        for (int j = 0; j < IPT / 2; ++j) {
-            const int4 q = ld_stream16(p + 2 * j);
-            out[2 * j + 0] = (static_cast<int64_t>(static_cast<uint32_t>(q.y)) << 32) | static_cast<uint32_t>(q.x);
-            out[2 * j + 1] = (static_cast<int64_t>(static_cast<uint32_t>(q.w)) << 32) | static_cast<uint32_t>(q.z);
-        }
-    } else {
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) out[e] = (base + e < r1) ? p[e] : 0;
-    }
-}
-
-template <typename VT, int IPT>
-__device__ __forceinline__ void load_vals(const void* col, int64_t base, bool full, int64_t r1, VT (&out)[IPT]) {
-    if constexpr (sizeof(VT) == 4) {
-        int32_t t[IPT];
-        load_i32<IPT>(col, base, full, r1, t);
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) memcpy(&out[e], &t[e], 4);
-    } else {
-        int64_t t[IPT];
-        load_i64<IPT>(col, base, full, r1, t);
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) memcpy(&out[e], &t[e], 8);
     }
 }
 
@@ -174,39 +137,75 @@ __device__ __forceinline__ int64_t pred_ord64(int64_t b, bool is_float) {
     return is_float ? (b ^ ((b >> 63) & 0x7fffffffffffffffll)) : b;
 }
 
-// ---------------------------------------------------------------------------------------------
-// One work item: rows [r0, r1) of query I, processed by one warp group.
-// ---------------------------------------------------------------------------------------------
-template <typename VT, int IPT>
-__device__ __forceinline__ void b_item(const BInst& I, int64_t r0, int64_t r1, unsigned char* gsm, int gtid,
-                                    int gthreads, int bar, unsigned long long* claims) {
-    constexpr bool V32 = sizeof(VT) == 4;
-    const int S = I.S;
-    const int RS = S * I.R;
-    const bool has_vals = I.vk != VK_NONE;
-    const bool has_sum = I.has_sum, has_min = I.has_min, has_max = I.has_max;
-    const bool has_mm = has_min || has_max;
-    const Layout L = I.L;
-    const int W = L.W;
-    const Region main = I.main;
-    unsigned long long* counters = I.counters;
 
+// ---------------------------------------------------------------------------------------------
+// Warp-group plumbing.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMetaFirst = 1;  // first tile of its item
+constexpr int kMetaLast = 2;   // last tile of its item
+constexpr int kMetaDone = 4;   // the queue is exhausted
+
+struct BStageMeta {
+    int32_t item;
+    int32_t flags;
+    int64_t r0;
+    int32_t nrows;
+    int32_t pad;
+};
+
+// The header of a warp group's shared memory.
+struct BGroupSmem {
+    uint64_t full[kBStages];
+    uint64_t empty[kBStages];
+    uint64_t csync;
+    uint64_t pad;
+    BStageMeta meta[kBStages];
+};
+static_assert(sizeof(BGroupSmem) <= kBHeaderBytes, "group header");
+
+// Column offsets inside one stage tile of `rows` rows.
+__device__ __forceinline__ int b_align128(int x) { return (x + 127) & ~127; }
+
+// Sync of the consumer warps of one group (mbarrier with one arrival per warp; bounded wait).
+__device__ __forceinline__ void b_csync(uint64_t* bar, uint32_t& parity, int32_t* err) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(bar);
+    b_wait(bar, parity, err);
+    parity ^= 1u;
+    __syncwarp();
+}
+
+// Shared-memory arrays of one query's tables inside the group's table region.
+__device__ __forceinline__ BSmem b_tables(unsigned char* base, const BInst& I, bool v32) {
+    const int RS = I.S * I.R;
+    const bool has_mm = I.has_min || I.has_max;
+    unsigned char* t0 = base + I.so_table;
     BSmem t;
-    t.key = reinterpret_cast<uint64_t*>(gsm);
+    t.key = reinterpret_cast<uint64_t*>(t0);
     size_t off = static_cast<size_t>(RS) * 8;
-    t.sum = reinterpret_cast<unsigned long long*>(gsm + off);
-    if (has_sum) off += static_cast<size_t>(RS) * 8;
-    t.mn = gsm + off;
-    t.mx = gsm + off;
+    t.sum = reinterpret_cast<unsigned long long*>(t0 + off);
+    if (I.has_sum) off += static_cast<size_t>(RS) * 8;
+    t.mn = t0 + off;
+    t.mx = t0 + off;
     if (has_mm) {
         off += static_cast<size_t>(RS) * 8;
-        if (!V32) {
-            t.mx = gsm + off;
+        if (!v32) {
+            t.mx = t0 + off;
             off += static_cast<size_t>(RS) * 8;
         }
     }
-    t.cnt = reinterpret_cast<unsigned int*>(gsm + off);
-    for (int i = gtid; i < RS; i += gthreads) {
+    t.cnt = reinterpret_cast<unsigned int*>(t0 + off);
+    return t;
+}
+
+template <typename VT>
+__device__ void b_clear(unsigned char* base, const BInst& I, int ctid, int cthreads) {
+    constexpr bool V32 = sizeof(VT) == 4;
+    const int RS = I.S * I.R;
+    if (RS == 0) return;
+    const BSmem t = b_tables(base, I, V32);
+    const bool has_sum = I.has_sum, has_mm = I.has_min || I.has_max;
+    for (int i = ctid; i < RS; i += cthreads) {
         t.key[i] = kEmpty;
         t.cnt[i] = 0u;
         if (has_sum) t.sum[i] = 0ull;
@@ -219,198 +218,390 @@ __device__ __forceinline__ void b_item(const BInst& I, int64_t r0, int64_t r1, u
             }
         }
     }
-    group_sync(bar, gthreads);
+}
 
-    // This warp's shared table (replica) as an offset into the arrays.
-    const int tb = (I.R > 1) ? ((gtid >> 5) % I.R) * S : 0;
-    BSmem mt = t;
-    mt.key += tb;
-    mt.sum += tb;
-    mt.cnt += tb;
-    mt.mn += static_cast<size_t>(tb) * 8;
-    mt.mx += static_cast<size_t>(tb) * 8;
-    const int shift = 32 - (31 - __clz(S > 0 ? S : 1));
-    const int probe = I.probe;
+// Merges one query's shared tables into its global table.
+template <typename VT>
+__device__ void b_flush(unsigned char* base, const BInst& I, int ctid, int cthreads, unsigned long long* claims) {
+    constexpr bool V32 = sizeof(VT) == 4;
+    const int RS = I.S * I.R;
+    if (RS == 0) return;
+    const BSmem t = b_tables(base, I, V32);
+    const bool has_vals = I.vk != VK_NONE;
+    const bool has_sum = I.has_sum, has_min = I.has_min, has_max = I.has_max, has_mm = has_min || has_max;
+    const bool vfloat = std::is_floating_point<VT>::value;
+    const Layout L = I.L;
+    const Region main = I.main;
+    for (int i = ctid; i < RS; i += cthreads) {
+        const uint64_t key = t.key[i];
+        if (key == kEmpty) continue;
+        uint64_t* slot = g_find(main, L.W, key, mix64(key), I.counters, claims);
+        if (!slot) continue;
+        const unsigned long long c = t.cnt[i];
+        const uint64_t sumbits = has_sum ? t.sum[i] : 0ull;
+        long long mn = 0, mx = 0;
+        if (has_mm) {
+            if (V32) {
+                const int* w = reinterpret_cast<const int*>(t.mn) + 2 * i;
+                mn = w[0];
+                mx = w[1];
+            } else {
+                mn = reinterpret_cast<const long long*>(t.mn)[i];
+                mx = reinterpret_cast<const long long*>(t.mx)[i];
+            }
+        }
+        if (has_vals) g_merge(slot, L, has_sum, has_min, has_max, V32, vfloat, c, sumbits, mn, mx);
+        else if (L.cnt >= 0) atomicAdd(reinterpret_cast<unsigned long long*>(slot + L.cnt), c);
+    }
+}
+
+// Probe rounds a lane runs for its rows together before it falls back to the full (sequential) probe.
+constexpr int kProbeRounds = 4;
+
+// Applies one query to one staged tile of nrows rows.  The tile is walked in steps of RPT rows per thread (row
+// ctid + u * cthreads of the step); in the global placement the RPT probe sequences of a step advance in rounds,
+// every round issuing the next probe load of all unresolved rows together, so a thread waits for the longest
+// sequence rather than the sum of them.
+template <typename VT, int RPT>
+__device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int voff, int poff, int nrows,
+                       unsigned char* tbase, int ctid, int cthreads, int wig, unsigned long long* claims) {
+    constexpr bool V32 = sizeof(VT) == 4;
+    const int S = I.S;
+    const bool has_vals = I.vk != VK_NONE;
+    const bool has_sum = I.has_sum, has_min = I.has_min, has_max = I.has_max;
+    const Layout L = I.L;
+    const int W = L.W;
+    const Region main = I.main;
     const bool k32 = I.kt == 4;
     const int64_t kmod = I.key_mod;
     const int pbytes = I.pbytes;
     const bool pfloat = I.pfloat != 0, pinv = I.pinv != 0;
     const int64_t plo = I.plo, phi = I.phi;
-
-    for (int64_t base = r0 + static_cast<int64_t>(gtid) * IPT; base < r1;
-         base += static_cast<int64_t>(gthreads) * IPT) {
-        const bool full = base + IPT <= r1;
-        uint64_t kw[IPT];
-        bool ok[IPT];
-        VT v[IPT];
-        if (k32) {
-            int32_t k[IPT];
-            load_i32<IPT>(I.keys, base, full, r1, k);
-            if (kmod > 0 && kmod <= INT_MAX) {
-                const int32_t m = static_cast<int32_t>(kmod);
+    BSmem t{};
+    int shift = 0, probe = 0;
+    if (S > 0) {
+        t = b_tables(tbase, I, V32);
+        const int tb = (I.R > 1) ? (wig % I.R) * S : 0;
+        t.key += tb;
+        t.sum += tb;
+        t.cnt += tb;
+        t.mn += static_cast<size_t>(tb) * 8;
+        t.mx += static_cast<size_t>(tb) * 8;
+        shift = 32 - (31 - __clz(S));
+        probe = I.probe;
+    }
+    for (int j0 = 0; j0 < nrows; j0 += RPT * cthreads) {
+        uint64_t kw[RPT];
+        VT v[RPT];
+        bool ok[RPT];
 #pragma unroll
-                for (int e = 0; e < IPT; ++e) k[e] = k[e] % m;
-            } else if (kmod > 0) {  // |k| < kmod except INT32_MIN % 2^31
-#pragma unroll
-                for (int e = 0; e < IPT; ++e) k[e] = static_cast<int32_t>(static_cast<int64_t>(k[e]) % kmod);
+        for (int u = 0; u < RPT; ++u) {
+            const int j = j0 + ctid + u * cthreads;
+            ok[u] = j < nrows;
+            kw[u] = 0;
+            v[u] = VT{};
+            if (!ok[u]) continue;
+            if (k32) {
+                int32_t k = reinterpret_cast<const int32_t*>(st + koff)[j];
+                if (kmod > 0) {
+                    if (kmod <= INT_MAX) k = k % static_cast<int32_t>(kmod);
+                    else k = static_cast<int32_t>(static_cast<int64_t>(k) % kmod);  // |k| < kmod except INT32_MIN
+                }
+                kw[u] = key_word(k);
+            } else {
+                int64_t k = reinterpret_cast<const int64_t*>(st + koff)[j];
+                if (kmod > 0) k = k % kmod;
+                kw[u] = key_word(k);
             }
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) kw[e] = key_word(k[e]);
-        } else {
-            int64_t k[IPT];
-            load_i64<IPT>(I.keys, base, full, r1, k);
-            if (kmod > 0) {
-#pragma unroll
-                for (int e = 0; e < IPT; ++e) k[e] = k[e] % kmod;
-            }
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) kw[e] = key_word(k[e]);
-        }
-        if (has_vals) load_vals<VT, IPT>(I.vals, base, full, r1, v);
-        else {
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) v[e] = VT{};
-        }
-#pragma unroll
-        for (int e = 0; e < IPT; ++e) ok[e] = full || base + e < r1;
-        if (pbytes == 4) {
-            int32_t p[IPT];
-            load_i32<IPT>(I.pcol, base, full, r1, p);
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) {
-                const int64_t o = pred_ord32(p[e], pfloat);
-                ok[e] = ok[e] && (((o >= plo) && (o <= phi)) != pinv);
-            }
-        } else if (pbytes == 8) {
-            int64_t p[IPT];
-            load_i64<IPT>(I.pcol, base, full, r1, p);
-#pragma unroll
-            for (int e = 0; e < IPT; ++e) {
-                const int64_t o = pred_ord64(p[e], pfloat);
-                ok[e] = ok[e] && (((o >= plo) && (o <= phi)) != pinv);
+            if (has_vals) v[u] = reinterpret_cast<const VT*>(st + voff)[j];
+            if (pbytes == 4) {
+                const int32_t b = reinterpret_cast<const int32_t*>(st + poff)[j];
+                const int64_t o = pfloat ? static_cast<int64_t>(b ^ ((b >> 31) & 0x7fffffff)) : static_cast<int64_t>(b);
+                ok[u] = ((o >= plo) && (o <= phi)) != pinv;
+            } else if (pbytes == 8) {
+                const int64_t b = reinterpret_cast<const int64_t*>(st + poff)[j];
+                const int64_t o = pfloat ? (b ^ ((b >> 63) & 0x7fffffffffffffffll)) : b;
+                ok[u] = ((o >= plo) && (o <= phi)) != pinv;
             }
         }
         if (S > 0) {
 #pragma unroll
-            for (int e = 0; e < IPT; ++e) {
-                if (!ok[e]) continue;
+            for (int u = 0; u < RPT; ++u) {
+                if (!ok[u]) continue;
                 int s = -1;
-                if (kw[e] != kEmpty) {
+                if (kw[u] != kEmpty) {
                     bool found = false;
-                    s = s_find(mt.key, S, probe, kw[e], smem_hash(kw[e], shift), &found);
+                    s = s_find(t.key, S, probe, kw[u], smem_hash(kw[u], shift), &found);
                 }
                 if (s >= 0) {
-                    b_s_acc<VT>(mt, s, v[e], has_vals, has_sum, has_min, has_max);
+                    b_s_acc<VT>(t, s, v[u], has_vals, has_sum, has_min, has_max);
                 } else {
-                    uint64_t* slot = (kw[e] == kEmpty) ? g_special(main, W, 1, claims)
-                                                       : g_find(main, W, kw[e], mix64(kw[e]), counters, claims);
-                    if (slot) b_g_acc<VT>(slot, L, v[e], has_vals, has_sum, has_min, has_max);
+                    uint64_t* slot = (kw[u] == kEmpty) ? g_special(main, W, 1, claims)
+                                                       : g_find(main, W, kw[u], mix64(kw[u]), I.counters, claims);
+                    if (slot) b_g_acc<VT>(slot, L, v[u], has_vals, has_sum, has_min, has_max);
                 }
             }
         } else {
-            uint64_t sl[IPT], cur[IPT];
+            uint64_t pos[RPT], cur[RPT];
+            uint64_t* slot[RPT];
+            bool pend[RPT];
 #pragma unroll
-            for (int e = 0; e < IPT; ++e) {
-                sl[e] = mix64(kw[e]) & main.mask;
-                cur[e] = (ok[e] && kw[e] != kEmpty) ? ld_volatile_u64(main.slots + sl[e] * W) : 0ull;
+            for (int u = 0; u < RPT; ++u) {
+                pos[u] = mix64(kw[u]) & main.mask;
+                pend[u] = ok[u] && kw[u] != kEmpty;
+                slot[u] = nullptr;
+                cur[u] = pend[u] ? ld_volatile_u64(main.slots + pos[u] * W) : 0ull;
             }
+            for (int round = 0; round < kProbeRounds; ++round) {
+                bool any = false;
 #pragma unroll
-            for (int e = 0; e < IPT; ++e) {
-                if (!ok[e]) continue;
-                uint64_t* slot = (kw[e] == kEmpty) ? g_special(main, W, 1, claims)
-                                                   : g_find_from(main, W, kw[e], sl[e], cur[e], counters, claims);
-                if (slot) b_g_acc<VT>(slot, L, v[e], has_vals, has_sum, has_min, has_max);
-            }
-        }
-    }
-    group_sync(bar, gthreads);
-
-    // Merge the shared tables into the global table.
-    if (S > 0) {
-        const bool vfloat = std::is_floating_point<VT>::value;
-        for (int i = gtid; i < RS; i += gthreads) {
-            const uint64_t key = t.key[i];
-            if (key == kEmpty) continue;
-            uint64_t* slot = g_find(main, W, key, mix64(key), counters, claims);
-            if (!slot) continue;
-            const unsigned long long c = t.cnt[i];
-            const uint64_t sumbits = has_sum ? t.sum[i] : 0ull;
-            long long mn = 0, mx = 0;
-            if (has_mm) {
-                if (V32) {
-                    const int* w = reinterpret_cast<const int*>(t.mn) + 2 * i;
-                    mn = w[0];
-                    mx = w[1];
-                } else {
-                    mn = reinterpret_cast<const long long*>(t.mn)[i];
-                    mx = reinterpret_cast<const long long*>(t.mx)[i];
+                for (int u = 0; u < RPT; ++u) {
+                    if (!pend[u]) continue;
+                    uint64_t* sp = main.slots + pos[u] * W;
+                    if (cur[u] == kw[u]) {
+                        slot[u] = sp;
+                        pend[u] = false;
+                    } else if (cur[u] == kEmpty) {
+                        const unsigned long long prev =
+                            atomicCAS(reinterpret_cast<unsigned long long*>(sp), kEmpty, kw[u]);
+                        if (prev == kEmpty || prev == kw[u]) {
+                            if (prev == kEmpty) claim_counted(claims);
+                            slot[u] = sp;
+                            pend[u] = false;
+                        }
+                    }
+                    if (pend[u]) {
+                        pos[u] = (pos[u] + 1) & main.mask;
+                        any = true;
+                    }
                 }
+                if (!any) break;
+#pragma unroll
+                for (int u = 0; u < RPT; ++u)
+                    if (pend[u]) cur[u] = ld_volatile_u64(main.slots + pos[u] * W);
             }
-            if (has_vals) {
-                g_merge(slot, L, has_sum, has_min, has_max, V32, vfloat, c, sumbits, mn, mx);
-            } else if (L.cnt >= 0) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(slot + L.cnt), c);
+#pragma unroll
+            for (int u = 0; u < RPT; ++u) {
+                if (!ok[u]) continue;
+                if (kw[u] == kEmpty) slot[u] = g_special(main, W, 1, claims);
+                else if (pend[u]) slot[u] = g_find_from(main, W, kw[u], pos[u], cur[u], I.counters, claims);
+                if (slot[u]) b_g_acc<VT>(slot[u], L, v[u], has_vals, has_sum, has_min, has_max);
             }
         }
     }
-    group_sync(bar, gthreads);
-    if (gtid == 0) {
-        publish_claims(counters, static_cast<unsigned long long>(I.capacity), *claims);
-        *claims = 0;
+}
+
+template <typename VT>
+__device__ __forceinline__ void b_members_tile(const BGroup& grp, const BInst* desc, const unsigned char* st,
+                                               int koff, int voff, int poff, int nrows, unsigned char* tbase,
+                                               int ctid, int cthreads, int wig, int rpt, unsigned long long* claims) {
+    for (int k = 0; k < grp.n_members; ++k) {
+        switch (rpt) {
+            case 1: b_tile<VT, 1>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
+            case 2: b_tile<VT, 2>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
+            default: b_tile<VT, 4>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
+        }
     }
+}
+
+template <typename VT>
+__device__ __forceinline__ void b_members_clear(const BGroup& grp, const BInst* desc, unsigned char* tbase, int ctid,
+                                                int cthreads) {
+    for (int k = 0; k < grp.n_members; ++k) b_clear<VT>(tbase, desc[k], ctid, cthreads);
+}
+
+template <typename VT>
+__device__ __forceinline__ void b_members_flush(const BGroup& grp, const BInst* desc, unsigned char* tbase, int ctid,
+                                                int cthreads, unsigned long long* claims) {
+    for (int k = 0; k < grp.n_members; ++k) b_flush<VT>(tbase, desc[k], ctid, cthreads, claims + k);
+}
+
+// Copies the rows of [r, r + nrows) of one column that a bulk copy cannot move (the final < 16 bytes of an
+// unaligned tail) with plain loads; returns the bytes the bulk copy moves.
+__device__ __forceinline__ uint32_t b_tail(unsigned char* dst, const void* col, int elem, int64_t r, int nrows, int lane) {
+    const uint32_t bytes = static_cast<uint32_t>(nrows) * elem;
+    const uint32_t bulk = bytes & ~15u;
+    for (int j = static_cast<int>(bulk / elem) + lane; j < nrows; j += 32) {
+        if (elem == 4) reinterpret_cast<int32_t*>(dst)[j] = static_cast<const int32_t*>(col)[r + j];
+        else reinterpret_cast<int64_t*>(dst)[j] = static_cast<const int64_t*>(col)[r + j];
+    }
+    return bulk;
 }
 
 __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchArgs ba) {
     extern __shared__ __align__(128) unsigned char sm[];
-    __shared__ __align__(16) BInst s_inst[4];
-    __shared__ int s_idx[4];
-    __shared__ unsigned long long s_claims[4];
+    __shared__ unsigned long long s_claims[4][kBMaxMembers];
+    __shared__ __align__(16) BInst s_desc[4][kBMaxMembers];  // member descriptors of every group's current item
     const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    int32_t* err = &ba.hdr->error;
     for (int q = 0; q < kBQueues; ++q) {
         const int qb = ba.hdr->q_begin[q];
         const int qe = ba.hdr->q_begin[q + 1];
         if (qb >= qe) continue;
-        const int gw = kBWarps >> q;
-        const int g = warp / gw;
-        const int gthreads = gw * 32;
-        const int gtid = threadIdx.x - g * gthreads;
-        const int bar = 1 + g;
+        const int G = 1 << q;
+        const int cw = kBCons >> q;
         const size_t gbytes = (static_cast<size_t>(ba.dyn_bytes) >> q) & ~static_cast<size_t>(127);
-        unsigned char* gsm = sm + g * gbytes;
-        if (gtid == 0) s_claims[g] = 0;
-        for (;;) {
-            if (gtid == 0) s_idx[g] = qb + static_cast<int>(atomicAdd(&ba.hdr->heads[q], 1ull));
-            group_sync(bar, gthreads);
-            const int idx = s_idx[g];
-            if (idx >= qe) break;
-            const BItem it = ba.items[idx];
-            constexpr int kWords = static_cast<int>(sizeof(BInst) / 8);
-            if (gtid < kWords)
-                reinterpret_cast<uint64_t*>(&s_inst[g])[gtid] = reinterpret_cast<const uint64_t*>(ba.inst + it.inst)[gtid];
-            group_sync(bar, gthreads);
-            const unsigned long long t0 = global_ns();
-            const BInst& I = s_inst[g];
-            const bool wide = I.ipt == 8;
-            switch (I.vk) {
-                case VK_I64:
-                    if (wide) b_item<int64_t, 8>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    else b_item<int64_t, 4>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    break;
-                case VK_F32:
-                    if (wide) b_item<float, 8>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    else b_item<float, 4>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    break;
-                case VK_F64:
-                    if (wide) b_item<double, 8>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    else b_item<double, 4>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    break;
-                default:  // VK_I32 and tables without a value column
-                    if (wide) b_item<int32_t, 8>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    else b_item<int32_t, 4>(I, it.r0, it.r1, gsm, gtid, gthreads, bar, &s_claims[g]);
-                    break;
+        const int SB = b_stage_bytes(q);
+        // barriers of every group of this phase
+        if (threadIdx.x == 0) {
+            for (int g = 0; g < G; ++g) {
+                BGroupSmem* h = reinterpret_cast<BGroupSmem*>(sm + g * gbytes);
+                for (int s = 0; s < kBStages; ++s) {
+                    mbar_init(&h->full[s], 1);
+                    mbar_init(&h->empty[s], cw);
+                }
+                mbar_init(&h->csync, cw);
             }
-            if (gtid == 0) ba.item_ns[idx] = static_cast<long long>(global_ns() - t0);
-            group_sync(bar, gthreads);
+            mbar_fence_init();
+        }
+        if (threadIdx.x < 4 * kBMaxMembers) s_claims[threadIdx.x / kBMaxMembers][threadIdx.x % kBMaxMembers] = 0;
+        __syncthreads();
+
+        if (warp >= kBCons) {
+            // ---------------- producer warp of group g ----------------
+            const int g = warp - kBCons;
+            if (g < G) {
+                unsigned char* gsm = sm + g * gbytes;
+                BGroupSmem* h = reinterpret_cast<BGroupSmem*>(gsm);
+                unsigned char* ring = gsm + gbytes - b_ring_bytes(q);
+                const uint64_t pol = l2_evict_first_policy();
+                uint32_t seq = 0;
+                bool alive = true;
+                while (alive) {
+                    int idx = 0;
+                    if (lane == 0) idx = qb + static_cast<int>(atomicAdd(&ba.hdr->heads[q], 1ull));
+                    idx = __shfl_sync(0xffffffffu, idx, 0);
+                    if (idx >= qe) {
+                        const int s = static_cast<int>(seq % kBStages);
+                        if (seq >= kBStages && !b_wait(&h->empty[s], ((seq / kBStages) - 1) & 1u, err)) break;
+                        if (lane == 0) {
+                            h->meta[s].flags = kMetaDone;
+                            mbar_arrive(&h->full[s]);
+                        }
+                        break;
+                    }
+                    const BItem it = ba.items[idx];
+                    const BGroup& grp = ba.groups[it.group];
+                    const int T = grp.stage_rows;
+                    const int kt = grp.kt, vb = grp.vbytes, pb = grp.pbytes;
+                    const int koff = 0, voff = b_align128(T * kt), poff = voff + b_align128(T * vb);
+                    const void* kcol = grp.keys;
+                    const void* vcol = grp.vals;
+                    const void* pcol = grp.pcol;
+                    for (int64_t r = it.r0; r < it.r1; r += T) {
+                        const int s = static_cast<int>(seq % kBStages);
+                        if (seq >= kBStages && !b_wait(&h->empty[s], ((seq / kBStages) - 1) & 1u, err)) {
+                            alive = false;
+                            break;
+                        }
+                        const int nrows = static_cast<int>(min(static_cast<int64_t>(T), it.r1 - r));
+                        unsigned char* st = ring + s * SB;
+                        const uint32_t kbulk = b_tail(st + koff, kcol, kt, r, nrows, lane);
+                        const uint32_t vbulk = vb ? b_tail(st + voff, vcol, vb, r, nrows, lane) : 0u;
+                        const uint32_t pbulk = pb ? b_tail(st + poff, pcol, pb, r, nrows, lane) : 0u;
+                        __syncwarp();
+                        if (lane == 0) {
+                            BStageMeta& m = h->meta[s];
+                            m.item = idx;
+                            m.r0 = r;
+                            m.nrows = nrows;
+                            m.flags = (r == it.r0 ? kMetaFirst : 0) | (r + T >= it.r1 ? kMetaLast : 0);
+                            fence_proxy_async_smem();
+                            mbar_arrive_expect_tx(&h->full[s], kbulk + vbulk + pbulk);
+                            if (kbulk) bulk_g2s(st + koff, static_cast<const unsigned char*>(kcol) + r * kt, kbulk, &h->full[s], pol);
+                            if (vbulk) bulk_g2s(st + voff, static_cast<const unsigned char*>(vcol) + r * vb, vbulk, &h->full[s], pol);
+                            if (pbulk) bulk_g2s(st + poff, static_cast<const unsigned char*>(pcol) + r * pb, pbulk, &h->full[s], pol);
+                        }
+                        __syncwarp();
+                        ++seq;
+                    }
+                }
+                // Every issued stage must be consumed (no copy in flight) before the phase ends.
+                for (uint32_t d = (seq > kBStages ? seq - kBStages : 0); d < seq; ++d)
+                    if (!b_wait(&h->empty[d % kBStages], (d / kBStages) & 1u, err)) break;
+            }
+        } else {
+            // ---------------- consumer warps of group g ----------------
+            const int g = warp / cw;
+            const int wig = warp - g * cw;
+            const int cthreads = cw * 32;
+            const int ctid = threadIdx.x - g * cthreads;
+            unsigned char* gsm = sm + g * gbytes;
+            BGroupSmem* h = reinterpret_cast<BGroupSmem*>(gsm);
+            unsigned char* tbase = gsm + kBHeaderBytes;
+            const unsigned char* ring = gsm + gbytes - b_ring_bytes(q);
+            unsigned long long* claims = s_claims[g];
+            uint32_t seq = 0, cpar = 0;
+            unsigned long long t0 = 0;
+            for (;;) {
+                const int s = static_cast<int>(seq % kBStages);
+                if (!b_wait(&h->full[s], (seq / kBStages) & 1u, err)) break;
+                const BStageMeta m = h->meta[s];
+                if (m.flags & kMetaDone) break;
+                const BItem it = ba.items[m.item];
+                const BGroup& grp = ba.groups[it.group];
+                const int T = grp.stage_rows;
+                const int koff = 0, voff = b_align128(T * grp.kt), poff = voff + b_align128(T * grp.vbytes);
+                const unsigned char* st = ring + s * SB;
+                const int vk = grp.vk;
+                BInst* desc = s_desc[g];
+                if (m.flags & kMetaFirst) {
+                    b_csync(&h->csync, cpar, err);  // the previous item's claims are published
+                    if (ctid == 0) t0 = global_ns();
+                    constexpr int kWords = static_cast<int>(sizeof(BInst) / 8);
+                    for (int w = ctid; w < grp.n_members * kWords; w += cthreads)
+                        reinterpret_cast<uint64_t*>(desc)[w] =
+                            reinterpret_cast<const uint64_t*>(ba.inst + grp.members[w / kWords])[w % kWords];
+                    b_csync(&h->csync, cpar, err);
+                    switch (vk) {
+                        case VK_I64: b_members_clear<int64_t>(grp, desc, tbase, ctid, cthreads); break;
+                        case VK_F32: b_members_clear<float>(grp, desc, tbase, ctid, cthreads); break;
+                        case VK_F64: b_members_clear<double>(grp, desc, tbase, ctid, cthreads); break;
+                        default: b_members_clear<int32_t>(grp, desc, tbase, ctid, cthreads); break;
+                    }
+                    b_csync(&h->csync, cpar, err);
+                }
+                const int rpt = grp.rpt;
+                switch (vk) {
+                    case VK_I64: b_members_tile<int64_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
+                    case VK_F32: b_members_tile<float>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
+                    case VK_F64: b_members_tile<double>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
+                    default: b_members_tile<int32_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&h->empty[s]);
+                if (m.flags & kMetaLast) {
+                    b_csync(&h->csync, cpar, err);
+                    switch (vk) {
+                        case VK_I64: b_members_flush<int64_t>(grp, desc, tbase, ctid, cthreads, claims); break;
+                        case VK_F32: b_members_flush<float>(grp, desc, tbase, ctid, cthreads, claims); break;
+                        case VK_F64: b_members_flush<double>(grp, desc, tbase, ctid, cthreads, claims); break;
+                        default: b_members_flush<int32_t>(grp, desc, tbase, ctid, cthreads, claims); break;
+                    }
+                    b_csync(&h->csync, cpar, err);
+                    if (ctid == 0) {
+                        for (int k = 0; k < grp.n_members; ++k) {
+                            const BInst& I = desc[k];
+                            publish_claims(I.counters, static_cast<unsigned long long>(I.capacity), claims[k]);
+                            claims[k] = 0;
+                        }
+                        ba.item_ns[m.item] = static_cast<long long>(global_ns() - t0);
+                    }
+                }
+                ++seq;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int g = 0; g < G; ++g) {
+                BGroupSmem* h = reinterpret_cast<BGroupSmem*>(sm + g * gbytes);
+                for (int s = 0; s < kBStages; ++s) {
+                    mbar_inval(&h->full[s]);
+                    mbar_inval(&h->empty[s]);
+                }
+                mbar_inval(&h->csync);
+            }
         }
         __syncthreads();
     }
@@ -585,6 +776,7 @@ __global__ void __launch_bounds__(kBResThreads) gb_batch_results_kernel(const Ba
     }
     if (threadIdx.x == 0) {
         int32_t st = static_cast<int32_t>(I.counters[1] & 0xffffffffull);
+        if (ba.hdr->error != QDB_OK) st = ba.hdr->error;
         if (done > cap && st == QDB_OK) st = QDB_HASH_TABLE_FULL;
         ba.res_count[i] = done < cap ? done : cap;
         ba.status[i] = st;

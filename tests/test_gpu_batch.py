@@ -144,11 +144,11 @@ def test_batch_graph_replays(cuda):
 
 
 PLANS = [
-    {"placement": capi.QDB_PLACE_GLOBAL, "warps": 16, "rows_per_thread": 4},
-    {"placement": capi.QDB_PLACE_GLOBAL, "warps": 4, "rows_per_thread": 8},
-    {"placement": capi.QDB_PLACE_SHARED, "replicas": 1, "warps": 16, "rows_per_thread": 8},
-    {"placement": capi.QDB_PLACE_SHARED, "replicas": 4, "warps": 8, "rows_per_thread": 4},
-    {"placement": capi.QDB_PLACE_SHARED, "replicas": 4, "warps": 4, "rows_per_thread": 8},
+    {"placement": capi.QDB_PLACE_GLOBAL, "warps": 12, "rows_per_thread": 4},
+    {"placement": capi.QDB_PLACE_GLOBAL, "warps": 3, "rows_per_thread": 1},
+    {"placement": capi.QDB_PLACE_SHARED, "replicas": 1, "warps": 12, "rows_per_thread": 2},
+    {"placement": capi.QDB_PLACE_SHARED, "replicas": 4, "warps": 6, "rows_per_thread": 4},
+    {"placement": capi.QDB_PLACE_SHARED, "replicas": 4, "warps": 3, "rows_per_thread": 1},
 ]
 
 
@@ -198,7 +198,7 @@ def test_batch_undersized_shared_table_spills_to_global(cuda):
     s = Spec(310, np.int32, np.int64, 500_000, 30_000, ["sum", "min", "max", "count"])
     b = GroupByBatch(1, 1 << 28, 1 << 26)
     b.set([s.query()])
-    b.set_cfg(0, placement=capi.QDB_PLACE_SHARED, smem_slots=256, replicas=2, warps=16, chunk_rows=65536)
+    b.set_cfg(0, placement=capi.QDB_PLACE_SHARED, smem_slots=256, replicas=2, warps=12, chunk_rows=65536)
     b.run()
     _, status = b.fetch()
     assert status[0] == 0
@@ -272,7 +272,7 @@ def test_batch_autotune(cuda):
     b.set([s.query() for s in specs])
     b.autotune()
     cfgs = [b.get_cfg(i) for i in range(len(specs))]
-    assert all(c["warps"] in (16, 8, 4) and c["rows_per_thread"] in (4, 8) for c in cfgs)
+    assert all(c["warps"] in (12, 6, 3) and c["rows_per_thread"] in (1, 2, 4) for c in cfgs)
     b.run()
     _, status = b.fetch()
     assert (status == 0).all()
@@ -303,3 +303,37 @@ def test_batch_rejects_bad_queries(cuda):
     with pytest.raises(QueryEngineError) as e:
         b.set([Query(k.float(), v, ["sum"], 10)])
     assert e.value.code == capi.QDB_ERR_INVALID
+
+
+@pytest.mark.parametrize("share", [True, False])
+def test_batch_shared_scan(cuda, share):
+    """Queries over the same columns (different WHERE constants, key moduli, aggregates, placements) aggregated in
+    shared scans: each result equals the oracle on that query alone."""
+    n = 600_000
+    k = dg.uniform_i64(400, 0, n, -(1 << 40), 1 << 40)
+    v = dg.lognormal_f32(400, 1, n, 2.0, 1.0)
+    p = dg.uniform_f32(400, 2, n)
+    dk, dv, dp = _dev(k), _dev(v), _dev(p)
+    specs = []
+    for i, (mod, sel, aggs) in enumerate([(10, 0.9, ["sum", "avg"]), (1000, 0.05, ["sum", "count", "max"]),
+                                          (7, 0.5, list(AGG_ORDER)), (100_000, 0.3, ["sum", "avg"]),
+                                          (64, 1.0, ["min", "count"]), (2, 0.01, ["sum"]),
+                                          (300, 0.7, ["max", "sum"]), (5000, 0.2, ["count"]),
+                                          (33, 0.6, ["sum", "avg", "count"]), (1 << 20, 0.4, ["sum", "count"])]):
+        s = Spec.__new__(Spec)
+        s.n, s.k, s.v, s.aggs, s.key_mod = n, k, v, aggs, mod
+        s.pred = (p, FilterConditions.less, sel, np.float32)
+        ek = np.fmod(k, mod)
+        keep = p < np.float32(sel)
+        s.max_groups = max(1, len(np.unique(ek[keep])))
+        s.ref = oracle.groupby(ek, v, pred=(p, FilterConditions.less, sel, np.float32, None))
+        s.dk, s.dv, s.dp = dk, dv, dp
+        specs.append(s)
+    b = GroupByBatch(len(specs), 1 << 30, 1 << 28)
+    b.set_sharing(share)
+    b.set([s.query() for s in specs])
+    b.run()
+    _, status = b.fetch()
+    assert (status == 0).all()
+    for s, r in zip(specs, b.results_all()):
+        s.check(r)
