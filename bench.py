@@ -58,7 +58,10 @@ def parse_args():
     ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served"])
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
     ap.add_argument("--plain-sample", type=int, default=0,
-                    help="batched: queries of the one-by-one plain-path comparison (0 = all)")
+                    help="batched / served: queries of the one-by-one plain-path comparison (0 = all / 24)")
+    ap.add_argument("--served-rows", type=int, default=1 << 30)
+    ap.add_argument("--served-queries", type=int, default=128)
+    ap.add_argument("--served-batch", type=int, default=32)
     return ap.parse_args()
 
 
@@ -554,6 +557,200 @@ def run_batched_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------------------------
+# Served workload: an open-loop Poisson stream of GROUP BY queries against 1B device-resident rows, continuously
+# batched by the serving loop, against the same queries issued one by one through the plain path.
+# ---------------------------------------------------------------------------------------------------------------
+SERVE_SEED = 20240603
+SERVE_METRIC = "served GROUP BY queries/s"
+SERVE_WORKLOAD = ("served-1B: open-loop Poisson query stream at 4 rates against 2^30 device-resident rows (int32 key "
+                  "uniform, int64 key uniform, f32 predicate U[0,1), f32 lognormal(2,1) value; 20 GB); queries of "
+                  "the shapes GROUP BY k32 % c: SUM+MIN+MAX+COUNT | k64 % c: SUM+AVG | k64 % c: SUM+COUNT+MAX, "
+                  "WHERE p < s with s uniform in [0.01, 1], c log-uniform in [10, 1M]; table admission budget 40 GB")
+SERVE_SHAPES = (("k32", ("sum", "min", "max", "count")), ("k64", ("sum", "avg")), ("k64", ("sum", "count", "max")))
+
+
+def served_columns(n: int, dev):
+    """The resident columns, generated in chunks on the host (seeded) and copied into device buffers."""
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    cols = {"k32": torch.empty(n, dtype=torch.int32, device=dev), "k64": torch.empty(n, dtype=torch.int64, device=dev),
+            "p": torch.empty(n, dtype=torch.float32, device=dev), "v": torch.empty(n, dtype=torch.float32, device=dev)}
+    chunk = 1 << 26
+    st = {k: torch.empty(chunk, dtype=v.dtype, pin_memory=True) for k, v in cols.items()}
+    for c0 in range(0, n, chunk):
+        m = min(chunk, n - c0)
+        part = c0 // chunk
+        dg.uniform_i32(SERVE_SEED, 4 * part + 0, m, 0, (1 << 31) - 1, out=st["k32"].numpy())
+        dg.uniform_i64(SERVE_SEED, 4 * part + 1, m, 0, 1 << 62, out=st["k64"].numpy())
+        dg.uniform_f32(SERVE_SEED, 4 * part + 2, m, out=st["p"].numpy())
+        dg.lognormal_f32(SERVE_SEED, 4 * part + 3, m, 2.0, 1.0, out=st["v"].numpy())
+        for k in cols:
+            cols[k][c0:c0 + m].copy_(st[k][:m])
+        torch.cuda.synchronize(dev)
+    return cols
+
+
+def served_queries(cols, n_q: int, seed: int):
+    from qikkdb_b200.batch import Query
+    from qikkdb_b200.groupby import FilterConditions
+    from qikkdb_b200 import datagen as dg
+    card = dg.loguniform_i64(seed, 0, n_q, 10, 1_000_000)
+    sel = dg.uniform_f32(seed, 1, n_q, 0.01, 1.0)
+    shape = dg.uniform_i32(seed, 2, n_q, 0, len(SERVE_SHAPES) - 1)
+    out = []
+    for i in range(n_q):
+        kc, aggs = SERVE_SHAPES[int(shape[i])]
+        out.append(Query(cols[kc], cols["v"], list(aggs), 0, key_mod=int(card[i]),
+                         pred=(cols["p"], FilterConditions.less, float(sel[i]), np.float32)))
+    return out
+
+
+def run_served(args):
+    import ctypes as C
+
+    import torch
+
+    from qikkdb_b200 import _capi
+    from qikkdb_b200.groupby import AGG_CODES
+    from qikkdb_b200.serve import Server, percentile_ms, poisson_arrivals
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = _capi.lib()
+    n = args.served_rows
+    cols = served_columns(n, dev)
+    srv = Server(max_batch=args.served_batch, in_flight=2, table_budget=40 << 30, result_budget=4 << 30)
+    n_q = args.served_queries
+    # warm-up, then capacity: every query of a closed burst submitted at once
+    warm = served_queries(cols, 16, SERVE_SEED + 99)
+    srv.run_open_loop(warm, np.zeros(len(warm), np.int64))
+    burst = served_queries(cols, n_q, SERVE_SEED + 1)
+    launches0 = lib.qdb_launch_count()
+    sampler = ClockSampler(local)
+    with sampler:
+        lat, stat, wall = srv.run_open_loop(burst, np.zeros(n_q, np.int64))
+    launches = lib.qdb_launch_count() - launches0
+    assert (stat == 0).all(), f"served queries failed: {np.unique(stat)}"
+    capacity = n_q / (wall / 1e9)
+    rates = []
+    for k, frac in enumerate((0.25, 0.5, 0.75, 0.95)):
+        rate = capacity * frac
+        qs = served_queries(cols, n_q, SERVE_SEED + 10 + k)
+        lat, stat, wall = srv.run_open_loop(qs, poisson_arrivals(rate, n_q, SERVE_SEED + 20 + k))
+        assert (stat == 0).all()
+        rates.append({"offered_qps": rate, "achieved_qps": n_q / (wall / 1e9), "p50_ms": percentile_ms(lat, 50),
+                      "p99_ms": percentile_ms(lat, 99), "queries": n_q})
+    st = srv.stats()
+    srv.close()
+
+    # the same kind of queries one by one through the plain path: key % c column (GPUBinary mod), table created
+    # with the query's true group bound, ProcessBlock with the fused WHERE, GetResults, results to host, free
+    plain = served_queries(cols, args.plain_sample or 24, SERVE_SEED + 1)
+    tmp = {"k32": torch.empty(n, dtype=torch.int32, device=dev), "k64": torch.empty(n, dtype=torch.int64, device=dev)}
+    s0 = torch.cuda.current_stream().cuda_stream
+    outs = (C.c_void_p * 8)()
+    onulls = (C.c_void_p * 8)()
+    okeys = (C.c_void_p * 1)()
+    oknull = (C.c_void_p * 1)()
+    cnt = C.c_int64()
+    from qikkdb_b200.groupby import make_pred
+
+    def plain_pass():
+        for q in plain:
+            kc = "k32" if q.keys.dtype == torch.int32 else "k64"
+            kt = _capi.QDB_INT32 if kc == "k32" else _capi.QDB_INT64
+            _capi.check(lib.qdb_arith_mod(kt, q.keys.data_ptr(), q.key_mod, tmp[kc].data_ptr(), n, s0))
+            mask = 0
+            for a in q.aggs:
+                mask |= AGG_CODES[a]
+            h = C.c_void_p()
+            _capi.check(lib.qdb_gb_create(C.byref(h), mask, kt, 1, _capi.QDB_FLOAT, min(q.key_mod, n), 0, s0))
+            p = make_pred(q.pred[0], q.pred[1], q.pred[2], q.pred[3])
+            kcol = (C.c_void_p * 1)(tmp[kc].data_ptr())
+            _capi.check(lib.qdb_gb_process_sync(h, kcol, None, q.vals.data_ptr(), None, n, C.byref(p), None, s0))
+            codes = (C.c_int32 * len(q.aggs))(*[AGG_CODES[a] for a in q.aggs])
+            _capi.check(lib.qdb_gb_results_multi(h, len(q.aggs), codes, okeys, oknull, outs, onulls, C.byref(cnt), s0))
+            g = cnt.value
+            host = np.empty(max(g, 1) * (1 + len(q.aggs)), np.int64)
+            if g:
+                _capi.check(lib.qdb_memcpy_d2h(host.ctypes.data, okeys[0], g * (4 if kc == "k32" else 8), s0))
+                for j, a in enumerate(q.aggs):  # COUNT is int64, the other aggregates of f32 values are float
+                    _capi.check(lib.qdb_memcpy_d2h(host.ctypes.data + 8 * g * (j + 1), outs[j],
+                                                   g * (8 if a == "count" else 4), s0))
+            lib.qdb_free(okeys[0], s0)
+            for j in range(len(q.aggs)):
+                lib.qdb_free(outs[j], s0)
+            lib.qdb_gb_destroy(h)
+        torch.cuda.synchronize(dev)
+
+    plain_pass_first = plain[:2]
+    saved = plain
+    plain = plain_pass_first
+    plain_pass()
+    plain = saved
+    t0 = time.perf_counter()
+    plain_pass()
+    plain_s = time.perf_counter() - t0
+    plain_qps = len(plain) / plain_s
+    peak, peak_kind = measured_peak()
+    line = {"metric": SERVE_METRIC, "value": capacity, "unit": "queries/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "replicas only",
+            "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "rows": n, "queries_per_rate": n_q, "max_batch": args.served_batch,
+                       "in_flight_batches": 2, "table_budget_bytes": 40 << 30,
+                       "tables": "sized by the server's cardinality estimate (sampled GEE, capped by the modulus)"},
+            "value_is": "closed-burst capacity: all queries submitted at t=0, queries / (first arrival to last result)",
+            "rates": rates,
+            "plain_one_by_one": {"value": plain_qps, "unit": "queries/s", "queries": len(plain), "seconds": plain_s,
+                                 "path": "per query: qdb_arith_mod (key % c column), qdb_gb_create (true bound), "
+                                         "qdb_gb_process_sync (fused WHERE), qdb_gb_results_multi, D2H, qdb_free"},
+            "speedup_vs_plain": capacity / plain_qps, "server_stats": st,
+            "e2e": {"value": capacity, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
+                    "path": "qdb_server_run_open_loop: results on the host per query; columns device-resident"},
+            "clocks": sampler.summary(), "gpu_launches": int(launches)}
+    print(json.dumps(line), flush=True)
+
+
+def run_served_reference(args):
+    """The oracle on a bounded sample of the served query stream (rows sampled from the same columns)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import oracle
+    from qikkdb_b200 import datagen as dg
+    rows = min(args.served_rows, 1 << 24)
+    k32 = dg.uniform_i32(SERVE_SEED, 0, rows, 0, (1 << 31) - 1)
+    k64 = dg.uniform_i64(SERVE_SEED, 1, rows, 0, 1 << 62)
+    p = dg.uniform_f32(SERVE_SEED, 2, rows)
+    v = dg.lognormal_f32(SERVE_SEED, 3, rows, 2.0, 1.0)
+    card = dg.loguniform_i64(SERVE_SEED + 1, 0, 64, 10, 1_000_000)
+    sel = dg.uniform_f32(SERVE_SEED + 1, 1, 64, 0.01, 1.0)
+    shape = dg.uniform_i32(SERVE_SEED + 1, 2, 64, 0, len(SERVE_SHAPES) - 1)
+    secs, done, threads = 0.0, 0, 0
+    for i in range(64):
+        k = k32 if SERVE_SHAPES[int(shape[i])][0] == "k32" else k64
+        r = oracle.groupby(np.fmod(k, int(card[i])), v, pred=(p, 2, float(sel[i]), np.float32, None), threads=0,
+                           sort=False, timing_only=True)
+        secs += r["seconds"]
+        threads = r["threads"]
+        done += 1
+        if secs > 20:
+            break
+    # scale the sampled rows to the full column length
+    value = done / (secs * args.served_rows / rows)
+    line = {"impl": "reference", "metric": SERVE_METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "replicas only",
+            "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "rows": args.served_rows},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "port",
+                             "sample": f"{done} queries of the stream over {rows} rows each (time scaled to "
+                                       f"{args.served_rows} rows), hash-map GROUP BY, {threads} threads, {secs:.1f} s"},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     if args.workload == "batched":
@@ -563,7 +760,11 @@ def main():
             run_batched(args)
         return
     if args.workload == "served":
-        from bench_served import run_served  # noqa: F401  (defined below when the served workload is built)
+        if args.impl == "reference":
+            run_served_reference(args)
+        else:
+            run_served(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

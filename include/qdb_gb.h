@@ -197,6 +197,11 @@ int32_t qdb_gb_merge_partial(qdb_gb* gb, const uint64_t* keys, const uint64_t* s
 int32_t qdb_filter(int32_t op, int32_t a_type, int32_t a_is_col, const void* a, int32_t b_type, int32_t b_is_col,
                    const void* b, const uint64_t* null_mask, int8_t* out_mask, int64_t n, void* stream);
 
+/* GPUBinary<ArithmeticOperations::mod, T, T*, T>::Binary (qikkDB/QueryEngine/GPUCore/GPUBinary.cuh:145-166) for a
+ * column and a constant: out[i] = in[i] % modulus (C++ remainder) for INT32 / INT64 columns; the `key % m` column
+ * the dispatcher materialises before a GROUP BY over that expression.  modulus 0 returns QDB_DIVISION_BY_ZERO. */
+int32_t qdb_arith_mod(int32_t type, const void* in, int64_t modulus, void* out, int64_t n, void* stream);
+
 /* ---- compaction: GPUReconstruct (qikkDB/QueryEngine/GPUCore/GPUReconstruct.cuh:204-355, :487-640) ----
  * qdb_reconstruct_keep: reconstructColKeep<T> with elem_bytes = sizeof(T) (1, 2, 4 or 8).  A NULL mask
  * returns `in` itself and n (no copy), as the reference does (GPUReconstruct.cuh:320-327).
@@ -256,7 +261,7 @@ typedef struct qdb_gb_query {
 typedef struct qdb_gb_batch_cfg {
     int32_t placement;       /* QDB_PLACE_SHARED: shared-memory tables merged into the global table at the end of
                                 every work item; QDB_PLACE_GLOBAL: every row goes to the global table */
-    int32_t smem_slots;      /* slots of one shared-memory table (a power of two >= 64), shared placement */
+    int32_t smem_slots;      /* slots of one shared-memory table (a multiple of 32, >= 64), shared placement */
     int32_t replicas;        /* shared-memory tables per warp group (warp w uses table w % replicas) */
     int32_t warps;           /* consumer warps cooperating on one work item: 12, 6 or 3 (1, 2 or 4 warp groups per
                                 CTA, each with its own producer warp and share of shared memory) */
@@ -316,6 +321,56 @@ int32_t qdb_gb_batch_required(const qdb_gb_query* queries, int32_t n, int64_t* t
 int32_t qdb_gb_batch_set_sharing(qdb_gb_batch* b, int32_t share);
 /* Clears the process-wide tuning table (plans fall back to the built-in heuristic). */
 int32_t qdb_gb_batch_tuning_reset(void);
+
+/* ---- serving loop: continuous batching of GROUP BY queries over device-resident columns ----
+ * No counterpart in the reference: its server hands every query to a dispatcher that runs the operators one
+ * query at a time per GPU (qikkDB/QueryEngine/GpuSqlDispatcher.cpp, TCPClientHandler).  Here queries are
+ * submitted from any thread and return at once with a ticket; one scheduler thread keeps up to `in_flight`
+ * batches on the GPU (each on its own stream, executed by the batch engine above, so their work overlaps on the
+ * device), admits pending queries in arrival order into the next free batch while their hash tables fit the
+ * table budget (table_budget_bytes over all batches in flight, split evenly between them) and their results
+ * fit the result budget, and on completion copies every query's results to host memory.  A query whose
+ * max_groups is 0 gets its table sized from a cardinality estimate (a sample of its key column, GEE estimator of
+ * Charikar, Chaudhuri, Motwani and Narasayya, PODS 2000, capped by key_mod); a query that reports
+ * QDB_HASH_TABLE_FULL is resubmitted with twice the table, like the dispatcher's restart on GPU_HASH_TABLE_FULL
+ * (GpuSqlDispatcherAggregationFunctions.h:452-470).  The columns must stay allocated until the query is done. */
+typedef struct qdb_server qdb_server; /* opaque serving loop */
+
+typedef struct qdb_server_result {
+    int32_t status;          /* QDB_OK, or the query's error */
+    int32_t n_cols;          /* aggregate columns (agg_mask bits in the order MIN, MAX, SUM, AVG, COUNT) */
+    int64_t n_groups;
+    const int64_t* keys;     /* host: n_groups keys as int64 (owned by the server until qdb_server_release) */
+    const int64_t* cols;     /* host: column j at cols + j * n_groups, 8-byte words as in qdb_gb_batch_result */
+    int64_t submit_ns;       /* steady-clock timestamps (ns) */
+    int64_t start_ns;        /* when its (last) batch was launched */
+    int64_t done_ns;         /* when its results were on the host */
+    int32_t retries;         /* resubmissions after HASH_TABLE_FULL */
+    int32_t batch_size;      /* queries in the batch that completed it */
+    int64_t max_groups;      /* table capacity it finally ran with */
+} qdb_server_result;
+
+typedef struct qdb_server_stats {
+    int64_t submitted, completed, batches, retries, rejected;
+    int64_t queries_in_batches; /* sum of batch sizes (mean batch size = queries_in_batches / batches) */
+} qdb_server_stats;
+
+int32_t qdb_server_create(qdb_server** out, int32_t max_batch, int32_t in_flight, int64_t table_budget_bytes,
+                          int64_t result_budget_bytes);
+/* Waits for the queries in flight, stops the scheduler and frees everything (tickets included). */
+int32_t qdb_server_destroy(qdb_server* s);
+/* Thread-safe; copies the query.  *ticket identifies it in qdb_server_wait / qdb_server_release. */
+int32_t qdb_server_submit(qdb_server* s, const qdb_gb_query* q, uint64_t* ticket);
+/* Blocks until the query is done or timeout_ms passes (QDB_ERR_TIMEOUT; timeout_ms < 0 waits for ever). */
+int32_t qdb_server_wait(qdb_server* s, uint64_t ticket, int64_t timeout_ms, qdb_server_result* out);
+/* Frees a finished ticket and its host results. */
+int32_t qdb_server_release(qdb_server* s, uint64_t ticket);
+int32_t qdb_server_stats_get(qdb_server* s, qdb_server_stats* out);
+/* Open-loop driver: submits queries[i] when arrival_ns[i] (ns after the call, non-decreasing) has come, whatever
+ * is still in flight, waits for all of them and writes latency_ns[i] = results on host - arrival time (so queueing
+ * delay counts) and status[i]; tickets are released.  *wall_ns = first arrival to last completion. */
+int32_t qdb_server_run_open_loop(qdb_server* s, const qdb_gb_query* queries, int32_t n, const int64_t* arrival_ns,
+                                 int64_t* latency_ns, int32_t* status, int64_t* wall_ns);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,27 @@ class qdb_gb_batch_cfg(C.Structure):
     ]
 
 
+class qdb_server_result(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("n_cols", C.c_int32),
+        ("n_groups", C.c_int64),
+        ("keys", C.c_void_p),
+        ("cols", C.c_void_p),
+        ("submit_ns", C.c_int64),
+        ("start_ns", C.c_int64),
+        ("done_ns", C.c_int64),
+        ("retries", C.c_int32),
+        ("batch_size", C.c_int32),
+        ("max_groups", C.c_int64),
+    ]
+
+
+class qdb_server_stats(C.Structure):
+    _fields_ = [(f, C.c_int64) for f in ("submitted", "completed", "batches", "retries", "rejected",
+                                         "queries_in_batches")]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 I32 = C.c_int32
@@ -112,6 +133,7 @@ SIGNATURES = [
     ("qdb_gb_export_partitioned", I32, [P, I32, PP, PP, PP, PI64, P]),
     ("qdb_gb_merge_partial", I32, [P, P, P, P, I64, P]),
     ("qdb_filter", I32, [I32, I32, I32, P, I32, I32, P, P, P, I64, P]),
+    ("qdb_arith_mod", I32, [I32, P, I64, P, I64, P]),
     ("qdb_reconstruct_keep", I32, [I32, P, P, I64, PP, PI64, P, PP, P]),
     ("qdb_reconstruct_keep_noalloc", I32, [I32, P, P, I64, P, I64, PI64, P, P, P]),
     ("qdb_generate_indexes", I32, [P, I64, PP, PI64, P]),
@@ -131,6 +153,13 @@ SIGNATURES = [
     ("qdb_gb_batch_required", I32, [C.POINTER(qdb_gb_query), I32, PI64, PI64]),
     ("qdb_gb_batch_set_sharing", I32, [P, I32]),
     ("qdb_gb_batch_tuning_reset", I32, []),
+    ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
+    ("qdb_server_destroy", I32, [P]),
+    ("qdb_server_submit", I32, [P, C.POINTER(qdb_gb_query), C.POINTER(C.c_uint64)]),
+    ("qdb_server_wait", I32, [P, C.c_uint64, I64, C.POINTER(qdb_server_result)]),
+    ("qdb_server_release", I32, [P, C.c_uint64]),
+    ("qdb_server_stats_get", I32, [P, C.POINTER(qdb_server_stats)]),
+    ("qdb_server_run_open_loop", I32, [P, C.POINTER(qdb_gb_query), I32, PI64, PI64, C.POINTER(I32), PI64]),
 ]
 
 _lib = None

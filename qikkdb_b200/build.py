@@ -28,6 +28,7 @@ NVCC_FLAGS = [
 CUDA_SOURCES = [
     "runtime.cu", "groupby.cu", "results.cu", "exchange.cu", "filter.cu", "reconstruct.cu", "hostpipe.cu",
     "agg_i32.cu", "agg_i64.cu", "agg_f32.cu", "agg_f64.cu", "agg_comp.cu", "batch.cu", "batch_kernels.cu",
+    "serve.cu",
 ]
 EXTRA_CUDA_SOURCES: list[str] = []
 

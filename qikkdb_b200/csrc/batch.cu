@@ -152,11 +152,13 @@ static qdb_gb_batch_cfg apply_kind(const qdb_gb_batch* b, const qdb_gb_query& q,
     c.placement = QDB_PLACE_GLOBAL;
     c.smem_slots = 0;
     c.replicas = 1;
-    const int64_t card = std::min<int64_t>(q.max_groups + 1, std::max<int64_t>(q.n_rows, 1));
+    const int64_t card = std::min<int64_t>(q.max_groups, std::max<int64_t>(q.n_rows, 1));
     if (k.place == QDB_PLACE_SHARED) {
         const size_t bps = smem_slot_bytes(q);
         const size_t gb = table_space(b, k.warps);
-        const int S = static_cast<int>(next_pow2_u(static_cast<uint64_t>(std::max<int64_t>(64, 2 * card))));
+        // load factor at most 0.625: short linear-probe runs, and as many queries as possible in shared memory
+        const int S = static_cast<int>(std::min<int64_t>((std::max<int64_t>(64, (card * 8 + 4) / 5) + 31) / 32 * 32,
+                                                         int64_t(1) << 20));
         int R = (k.rep == 0) ? 1 : (k.rep == 1 ? std::min(4, k.warps) : k.warps);
         while (R > 1 && align128(static_cast<size_t>(R) * S * bps) > gb) --R;
         if (align128(static_cast<size_t>(S) * bps) <= gb && S <= (1 << 20)) {
@@ -178,11 +180,11 @@ static qdb_gb_batch_cfg apply_kind(const qdb_gb_batch* b, const qdb_gb_query& q,
 
 static BKind heuristic_kind(const qdb_gb_query& q) {
     BKind k;
-    const int64_t card = std::min<int64_t>(q.max_groups + 1, std::max<int64_t>(q.n_rows, 1));
+    const int64_t card = std::min<int64_t>(q.max_groups, std::max<int64_t>(q.n_rows, 1));
     k.place = QDB_PLACE_SHARED;
-    k.rep = card <= 32 ? 2 : (card <= 512 ? 1 : 0);
-    k.warps = q.n_rows < 65536 ? kBCons / 4 : (q.n_rows < 524288 ? kBCons / 2 : kBCons);
-    k.rpt = 2;
+    k.rep = card <= 64 ? 2 : (card <= 512 ? 1 : 0);
+    k.warps = q.n_rows < 32768 ? kBCons / 4 : (q.n_rows < 262144 ? kBCons / 2 : kBCons);
+    k.rpt = card <= 4096 ? 1 : 2;
     return k;
 }
 
@@ -203,8 +205,10 @@ static int64_t result_words(const qdb_gb_query& q) {
 static int stage_rows(int warps, int kt, int vb, int pb) {
     const int q = queue_of(warps);
     auto bytes = [&](int t) { return align128(size_t(t) * kt) + align128(size_t(t) * vb) + align128(size_t(t) * pb); };
+    // every consumer warp compacts at most kBListRows rows of a tile (its share rounded up to 32 rows)
+    const int max_rows = (kBListRows - 32) * warps;
     int T = 128;
-    while (bytes(T + 128) <= static_cast<size_t>(b_stage_bytes(q))) T += 128;
+    while (T + 128 <= max_rows && bytes(T + 128) <= static_cast<size_t>(b_stage_bytes(q))) T += 128;
     return T;
 }
 
@@ -276,8 +280,10 @@ static int32_t build_items(qdb_gb_batch* b) {
         for (int k = 0; k < G.n_members; ++k) G.members[k] = members[gi][k];
         G.stage_rows = stage_rows(c.warps, G.kt, G.vbytes, G.pbytes);
         G.rpt = c.rows_per_thread;
+        // a shared scan does the work of every member per row: shorter items keep the queue balanced
         int64_t chunk = c.chunk_rows;
         for (int m : members[gi]) chunk = std::min<int64_t>(chunk, b->cfg[m].chunk_rows);
+        chunk = std::max<int64_t>(4096, (chunk / G.n_members + 63) / 64 * 64);
         const int qi = queue_of(c.warps);
         for (int64_t r = 0; r < q.n_rows; r += chunk) {
             BItem it{};
@@ -291,8 +297,8 @@ static int32_t build_items(qdb_gb_batch* b) {
     b->items.clear();
     for (int qi = 0; qi < kBQueues; ++qi) {
         // Longest items first, so the queue's tail is made of short items.
-        std::stable_sort(its[qi].begin(), its[qi].end(),
-                         [](const BItem& x, const BItem& y) { return (x.r1 - x.r0) > (y.r1 - y.r0); });
+        auto work = [&](const BItem& x) { return (x.r1 - x.r0) * b->h_groups[x.group].n_members; };
+        std::stable_sort(its[qi].begin(), its[qi].end(), [&](const BItem& x, const BItem& y) { return work(x) > work(y); });
         b->h_hdr->q_begin[qi] = static_cast<int32_t>(b->items.size());
         b->items.insert(b->items.end(), its[qi].begin(), its[qi].end());
     }
@@ -401,7 +407,7 @@ static int32_t check_cfg(const qdb_gb_batch* b, const qdb_gb_query& q, const qdb
     if (c.chunk_rows < 64 || c.chunk_rows % 64) return fail(QDB_ERR_INVALID, "batch cfg: chunk_rows must be a positive multiple of 64");
     if (c.placement == QDB_PLACE_SHARED) {
         const int S = c.smem_slots;
-        if (S < 64 || (S & (S - 1))) return fail(QDB_ERR_INVALID, "batch cfg: smem_slots must be a power of two >= 64");
+        if (S < 64 || (S % 32)) return fail(QDB_ERR_INVALID, "batch cfg: smem_slots must be a multiple of 32, >= 64");
         if (c.replicas < 1 || c.replicas > c.warps) return fail(QDB_ERR_INVALID, "batch cfg: replicas must be in [1, warps]");
         if (query_table_bytes(q, c) > table_space(b, c.warps))
             return fail(QDB_ERR_TOO_LARGE, "batch cfg: shared-memory tables do not fit the warp group");
@@ -452,6 +458,28 @@ static int32_t run_once(qdb_gb_batch* b, bool use_graph, cudaStream_t s) {
     note_launch(3);
     b->needs_init = false;
     return QDB_OK;
+}
+
+int32_t batch_check_query(const qdb_gb_query& q) { return check_query(q); }
+
+// Readback of a run for callers inside the library (the serving loop): enqueues, without synchronising, the
+// copies of every query's group count and status and of the whole result region to host buffers.
+int32_t batch_enqueue_readback(qdb_gb_batch* b, int64_t* h_counts, int32_t* h_status, void* h_res, int64_t h_res_bytes,
+                               cudaStream_t s) {
+    if (b->n == 0) return QDB_OK;
+    const int64_t bytes = (b->h_inst[b->n - 1].res_off + result_words(b->q[b->n - 1])) * 8;
+    if (bytes > h_res_bytes) return fail(QDB_ERR_TOO_LARGE, "batch readback: host result buffer too small");
+    QDB_CUDA_TRY(cudaMemcpyAsync(h_counts, b->d_res_count, b->n * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    QDB_CUDA_TRY(cudaMemcpyAsync(h_status, b->d_status, b->n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    QDB_CUDA_TRY(cudaMemcpyAsync(h_res, b->d_res, bytes, cudaMemcpyDeviceToHost, s));
+    return QDB_OK;
+}
+
+// Where query i's results sit in the result region: first word, rows reserved per column, aggregate columns.
+void batch_result_place(const qdb_gb_batch* b, int i, int64_t* off_words, int64_t* cap_rows, int32_t* n_cols) {
+    *off_words = b->h_inst[i].res_off;
+    *cap_rows = b->h_inst[i].res_cap;
+    *n_cols = __builtin_popcount(static_cast<unsigned>(b->h_inst[i].aggs));
 }
 
 }  // namespace qdb
@@ -585,6 +613,12 @@ int32_t qdb_gb_batch_set(qdb_gb_batch* b, const qdb_gb_query* queries, int32_t n
         I.main.mask = cap - 1;
         I.n = q.n_rows;
         I.key_mod = q.key_mod;
+        if (q.key_mod > 0) {
+            const ModMagic mm = mod_magic(static_cast<uint64_t>(q.key_mod));
+            I.mod_m = mm.m;
+            I.mod_s1 = mm.s1;
+            I.mod_s2 = mm.s2;
+        }
         I.capacity = q.max_groups;
         I.res_off = roff[i] / 8;
         I.res_cap = q.max_groups + 2;

@@ -14,6 +14,7 @@ constexpr int kBStageBytes = 24 * 1024;             // stage bytes at one group 
 constexpr int kBHeaderBytes = 256;                  // mbarriers and stage metadata of one warp group
 constexpr int kBMaxMembers = 8;                     // queries sharing one scan of their columns
 constexpr int kBMaxRowsPerLane = 4;
+constexpr int kBListRows = 256;                     // rows of a stage tile one consumer warp compacts (u16 list)
 constexpr int kBSmemCap = 192 * 1024;              // shared memory per CTA: the rest stays L1 for the probe loads
 constexpr int kBResThreads = 256;
 constexpr int kBResPer = 16;
@@ -41,10 +42,13 @@ struct BInst {
     int32_t pinv;                  // keep = (lo <= x <= hi) != pinv
     int32_t has_sum, has_min, has_max;
     int32_t aggs;
-    int32_t S;                     // slots of one shared-memory table (power of two), 0 = global placement
+    int32_t S;                     // slots of one shared-memory table (a multiple of 32), 0 = global placement
     int32_t R;                     // shared-memory tables of this query per warp group
     int32_t probe;                 // shared-memory probe limit
     int32_t so_table;              // byte offset of this query's shared tables in the group's table region
+    int32_t mod_s1;                // key modulus as multiply-high constants (mod_magic of key_mod)
+    uint64_t mod_m;
+    int32_t mod_s2;
     int32_t pad;
 };
 static_assert(sizeof(BInst) % 8 == 0, "BInst is 64-bit aligned");
@@ -94,5 +98,11 @@ struct BatchArgs {
     long long* item_ns;   // per item: device time of the item (globaltimer)
     int64_t dyn_bytes;    // dynamic shared memory of the aggregation kernel
 };
+
+// Host-side helpers of the batch for the serving loop (batch.cu).
+int32_t batch_check_query(const qdb_gb_query& q);
+int32_t batch_enqueue_readback(qdb_gb_batch* b, int64_t* h_counts, int32_t* h_status, void* h_res, int64_t h_res_bytes,
+                               cudaStream_t s);
+void batch_result_place(const qdb_gb_batch* b, int i, int64_t* off_words, int64_t* cap_rows, int32_t* n_cols);
 
 }  // namespace qdb

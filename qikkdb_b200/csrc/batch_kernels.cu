@@ -255,17 +255,42 @@ __device__ void b_flush(unsigned char* base, const BInst& I, int ctid, int cthre
     }
 }
 
+// Shared-memory probe of a table of any S slots: the 32-bit multiplicative hash of the folded key is mapped to
+// [0, S) by a multiply-high (Lemire's range reduction), then linear probing with wrap-around.  Returns the slot or
+// -1 after P probes.
+__device__ __forceinline__ int b_s_find(uint64_t* skey, int S, int P, uint64_t key) {
+    const uint32_t f = static_cast<uint32_t>(key) ^ static_cast<uint32_t>(key >> 32);
+    int s = static_cast<int>(__umulhi(f * 0x9e3779b1u, static_cast<uint32_t>(S)));
+    for (int p = 0; p < P; ++p) {
+        const uint64_t cur = *reinterpret_cast<volatile uint64_t*>(&skey[s]);
+        if (cur == key) return s;
+        if (cur == kEmpty) {
+            const unsigned long long prev = atomicCAS(reinterpret_cast<unsigned long long*>(&skey[s]), kEmpty, key);
+            if (prev == kEmpty || prev == key) return s;
+        }
+        s = (s + 1 == S) ? 0 : s + 1;
+    }
+    return -1;
+}
+
 // Probe rounds a lane runs for its rows together before it falls back to the full (sequential) probe.
 constexpr int kProbeRounds = 4;
 
-// Applies one query to one staged tile of nrows rows.  The tile is walked in steps of RPT rows per thread (row
-// ctid + u * cthreads of the step); in the global placement the RPT probe sequences of a step advance in rounds,
-// every round issuing the next probe load of all unresolved rows together, so a thread waits for the longest
+// Applies one query to one staged tile of nrows rows.  Consumer warp wig of the group takes a contiguous share of
+// the tile's rows.  Phase A evaluates the WHERE interval and compacts the passing rows' indices into the warp's
+// list with ballots (so rows that fail cost nothing later); phase B walks the list in steps of RPT rows per lane:
+// key (and key modulus), value, insert.  In the global placement the RPT probe sequences of a step advance in
+// rounds, every round issuing the next probe load of all unresolved rows together, so a lane waits for the longest
 // sequence rather than the sum of them.
 template <typename VT, int RPT>
 __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int voff, int poff, int nrows,
-                       unsigned char* tbase, int ctid, int cthreads, int wig, unsigned long long* claims) {
+                       unsigned char* tbase, int wig, int cw, uint16_t* list, unsigned long long* claims) {
     constexpr bool V32 = sizeof(VT) == 4;
+    const int lane = threadIdx.x & 31;
+    const int per_warp = (((nrows + cw - 1) / cw) + 31) & ~31;
+    const int r0 = wig * per_warp;
+    const int r1 = min(nrows, r0 + per_warp);
+    if (r0 >= r1) return;
     const int S = I.S;
     const bool has_vals = I.vk != VK_NONE;
     const bool has_sum = I.has_sum, has_min = I.has_min, has_max = I.has_max;
@@ -273,12 +298,41 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
     const int W = L.W;
     const Region main = I.main;
     const bool k32 = I.kt == 4;
-    const int64_t kmod = I.key_mod;
+    const bool kmod = I.key_mod > 0;
+    const uint64_t md = static_cast<uint64_t>(I.key_mod), mm = I.mod_m;
+    const int ms1 = I.mod_s1, ms2 = I.mod_s2;
     const int pbytes = I.pbytes;
-    const bool pfloat = I.pfloat != 0, pinv = I.pinv != 0;
-    const int64_t plo = I.plo, phi = I.phi;
+
+    // ---- phase A: compact the rows passing the WHERE interval
+    int count = r1 - r0;
+    if (pbytes) {
+        const bool pfloat = I.pfloat != 0, pinv = I.pinv != 0;
+        const int64_t plo = I.plo, phi = I.phi;
+        const uint32_t lt = (1u << lane) - 1u;
+        count = 0;
+        for (int j0 = r0; j0 < r1; j0 += 32) {
+            const int j = j0 + lane;
+            bool keep = j < r1;
+            if (keep) {
+                int64_t o;
+                if (pbytes == 4) {
+                    const int32_t b = reinterpret_cast<const int32_t*>(st + poff)[j];
+                    o = pfloat ? static_cast<int64_t>(b ^ ((b >> 31) & 0x7fffffff)) : static_cast<int64_t>(b);
+                } else {
+                    const int64_t b = reinterpret_cast<const int64_t*>(st + poff)[j];
+                    o = pfloat ? (b ^ ((b >> 63) & 0x7fffffffffffffffll)) : b;
+                }
+                keep = ((o >= plo) && (o <= phi)) != pinv;
+            }
+            const uint32_t bal = __ballot_sync(0xffffffffu, keep);
+            if (keep) list[count + __popc(bal & lt)] = static_cast<uint16_t>(j);
+            count += __popc(bal);
+        }
+        __syncwarp();
+    }
+
     BSmem t{};
-    int shift = 0, probe = 0;
+    int probe = 0;
     if (S > 0) {
         t = b_tables(tbase, I, V32);
         const int tb = (I.R > 1) ? (wig % I.R) * S : 0;
@@ -287,52 +341,32 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
         t.cnt += tb;
         t.mn += static_cast<size_t>(tb) * 8;
         t.mx += static_cast<size_t>(tb) * 8;
-        shift = 32 - (31 - __clz(S));
         probe = I.probe;
     }
-    for (int j0 = 0; j0 < nrows; j0 += RPT * cthreads) {
+    // ---- phase B: the passing rows, RPT per lane per step
+    for (int e0 = 0; e0 < count; e0 += RPT * 32) {
         uint64_t kw[RPT];
         VT v[RPT];
         bool ok[RPT];
 #pragma unroll
         for (int u = 0; u < RPT; ++u) {
-            const int j = j0 + ctid + u * cthreads;
-            ok[u] = j < nrows;
+            const int e = e0 + u * 32 + lane;
+            ok[u] = e < count;
             kw[u] = 0;
             v[u] = VT{};
             if (!ok[u]) continue;
-            if (k32) {
-                int32_t k = reinterpret_cast<const int32_t*>(st + koff)[j];
-                if (kmod > 0) {
-                    if (kmod <= INT_MAX) k = k % static_cast<int32_t>(kmod);
-                    else k = static_cast<int32_t>(static_cast<int64_t>(k) % kmod);  // |k| < kmod except INT32_MIN
-                }
-                kw[u] = key_word(k);
-            } else {
-                int64_t k = reinterpret_cast<const int64_t*>(st + koff)[j];
-                if (kmod > 0) k = k % kmod;
-                kw[u] = key_word(k);
-            }
+            const int j = pbytes ? static_cast<int>(list[e]) : r0 + e;
+            int64_t k = k32 ? static_cast<int64_t>(reinterpret_cast<const int32_t*>(st + koff)[j])
+                            : reinterpret_cast<const int64_t*>(st + koff)[j];
+            if (kmod) k = mod_signed(k, md, mm, ms1, ms2);
+            kw[u] = k32 ? key_word(static_cast<int32_t>(k)) : key_word(k);
             if (has_vals) v[u] = reinterpret_cast<const VT*>(st + voff)[j];
-            if (pbytes == 4) {
-                const int32_t b = reinterpret_cast<const int32_t*>(st + poff)[j];
-                const int64_t o = pfloat ? static_cast<int64_t>(b ^ ((b >> 31) & 0x7fffffff)) : static_cast<int64_t>(b);
-                ok[u] = ((o >= plo) && (o <= phi)) != pinv;
-            } else if (pbytes == 8) {
-                const int64_t b = reinterpret_cast<const int64_t*>(st + poff)[j];
-                const int64_t o = pfloat ? (b ^ ((b >> 63) & 0x7fffffffffffffffll)) : b;
-                ok[u] = ((o >= plo) && (o <= phi)) != pinv;
-            }
         }
         if (S > 0) {
 #pragma unroll
             for (int u = 0; u < RPT; ++u) {
                 if (!ok[u]) continue;
-                int s = -1;
-                if (kw[u] != kEmpty) {
-                    bool found = false;
-                    s = s_find(t.key, S, probe, kw[u], smem_hash(kw[u], shift), &found);
-                }
+                const int s = (kw[u] != kEmpty) ? b_s_find(t.key, S, probe, kw[u]) : -1;
                 if (s >= 0) {
                     b_s_acc<VT>(t, s, v[u], has_vals, has_sum, has_min, has_max);
                 } else {
@@ -389,17 +423,18 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
             }
         }
     }
+    __syncwarp();  // the list is reused by the next query of the scan group
 }
 
 template <typename VT>
 __device__ __forceinline__ void b_members_tile(const BGroup& grp, const BInst* desc, const unsigned char* st,
                                                int koff, int voff, int poff, int nrows, unsigned char* tbase,
-                                               int ctid, int cthreads, int wig, int rpt, unsigned long long* claims) {
+                                               int wig, int cw, uint16_t* list, int rpt, unsigned long long* claims) {
     for (int k = 0; k < grp.n_members; ++k) {
         switch (rpt) {
-            case 1: b_tile<VT, 1>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
-            case 2: b_tile<VT, 2>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
-            default: b_tile<VT, 4>(desc[k], st, koff, voff, poff, nrows, tbase, ctid, cthreads, wig, claims + k); break;
+            case 1: b_tile<VT, 1>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
+            case 2: b_tile<VT, 2>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
+            default: b_tile<VT, 4>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
         }
     }
 }
@@ -432,6 +467,7 @@ __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchA
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ unsigned long long s_claims[4][kBMaxMembers];
     __shared__ __align__(16) BInst s_desc[4][kBMaxMembers];  // member descriptors of every group's current item
+    __shared__ uint16_t s_list[kBCons][kBListRows];          // per consumer warp: passing rows of the tile
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     int32_t* err = &ba.hdr->error;
@@ -564,10 +600,10 @@ __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchA
                 }
                 const int rpt = grp.rpt;
                 switch (vk) {
-                    case VK_I64: b_members_tile<int64_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
-                    case VK_F32: b_members_tile<float>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
-                    case VK_F64: b_members_tile<double>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
-                    default: b_members_tile<int32_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, ctid, cthreads, wig, rpt, claims); break;
+                    case VK_I64: b_members_tile<int64_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
+                    case VK_F32: b_members_tile<float>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
+                    case VK_F64: b_members_tile<double>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
+                    default: b_members_tile<int32_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&h->empty[s]);

@@ -154,3 +154,43 @@ extern "C" int32_t qdb_filter(int32_t op, int32_t a_type, int32_t a_is_col, cons
         default: return fail(QDB_ERR_INVALID, "qdb_filter: unsupported left operand type");
     }
 }
+
+namespace qdb {
+
+// out[i] = in[i] % m (the C++ remainder): the expression column `key % m` that the dispatcher materialises with
+// GPUBinary<ArithmeticOperations::mod, T, T*, T> before a GROUP BY over it (GPUBinary.cuh:145-166).
+// The remainder uses the multiply-high form of the division by the invariant |m| (mod_signed, qdb_common.cuh);
+// a % m == a % |m| for C++'s truncating division.
+template <typename T>
+__global__ void mod_kernel(const T* __restrict__ in, ModMagic mm, T* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = static_cast<T>(mod_signed(static_cast<int64_t>(in[i]), mm.d, mm.m, mm.s1, mm.s2));
+}
+
+}  // namespace qdb
+
+extern "C" int32_t qdb_arith_mod(int32_t type, const void* in, int64_t modulus, void* out, int64_t n, void* stream) {
+    using namespace qdb;
+    if (n < 0 || (n > 0 && (!in || !out))) return fail(QDB_ERR_INVALID, "qdb_arith_mod: bad arguments");
+    if (modulus == 0) return fail(QDB_DIVISION_BY_ZERO, "qdb_arith_mod: modulo by zero");
+    if (n == 0) return QDB_OK;
+    cudaStream_t s = as_stream(stream);
+    const DeviceInfo& di = device_info();
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, int64_t(di.sm_count) * 16));
+    if (modulus == INT64_MIN) return fail(QDB_ERR_INVALID, "qdb_arith_mod: modulus out of range");
+    const ModMagic mm = mod_magic(static_cast<uint64_t>(modulus < 0 ? -modulus : modulus));
+    if (type == QDB_INT32) {
+        if (modulus > INT32_MAX || modulus < INT32_MIN)
+            return fail(QDB_ERR_INVALID, "qdb_arith_mod: modulus out of int32 range");
+        mod_kernel<int32_t><<<grid, 256, 0, s>>>(static_cast<const int32_t*>(in), mm, static_cast<int32_t*>(out), n);
+    } else if (type == QDB_INT64) {
+        mod_kernel<int64_t><<<grid, 256, 0, s>>>(static_cast<const int64_t*>(in), mm, static_cast<int64_t*>(out), n);
+    } else {
+        return fail(QDB_ERR_INVALID, "qdb_arith_mod: column must be INT32 or INT64");
+    }
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mod_kernel");
+    return QDB_OK;
+}

@@ -99,6 +99,48 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t k) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Remainder by an invariant divisor with one multiply-high: the unsigned division of Granlund and Montgomery,
+// "Division by Invariant Integers using Multiplication" (PLDI 1994), Figure 4.1 with N = 64.  For a divisor
+// 1 <= d < 2^63: l = ceil(log2 d), m = floor(2^64 (2^l - d) / d) + 1, and for every n < 2^64
+// q = (t + ((n - t) >> min(l, 1))) >> max(l - 1, 0) with t = mulhi(m, n).  The signed remainder follows C++
+// (the sign of the dividend), as GPUBinary's `a % b`.
+// ---------------------------------------------------------------------------------------------
+struct ModMagic {
+    uint64_t d = 1;
+    uint64_t m = 1;
+    int32_t s1 = 0;
+    int32_t s2 = 0;
+};
+
+inline ModMagic mod_magic(uint64_t d) {
+    ModMagic mm;
+    mm.d = d;
+    int l = 0;
+    while (l < 63 && (uint64_t(1) << l) < d) ++l;
+    const unsigned __int128 num = static_cast<unsigned __int128>((uint64_t(1) << l) - d) << 64;
+    mm.m = static_cast<uint64_t>(num / d) + 1;
+    mm.s1 = l < 1 ? l : 1;
+    mm.s2 = l > 1 ? l - 1 : 0;
+    return mm;
+}
+
+__host__ __device__ __forceinline__ uint64_t mulhi_u64(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return static_cast<uint64_t>((static_cast<unsigned __int128>(a) * b) >> 64);
+#endif
+}
+
+__host__ __device__ __forceinline__ int64_t mod_signed(int64_t k, uint64_t d, uint64_t m, int s1, int s2) {
+    const uint64_t u = k >= 0 ? static_cast<uint64_t>(k) : 0ull - static_cast<uint64_t>(k);
+    const uint64_t t = mulhi_u64(m, u);
+    const uint64_t q = (t + ((u - t) >> s1)) >> s2;
+    const uint64_t r = u - q * d;
+    return k >= 0 ? static_cast<int64_t>(r) : -static_cast<int64_t>(r);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Order-preserving integer encodings of IEEE floats, so MIN/MAX use native signed-integer atomics.
 // enc(x) < enc(y) iff x < y for non-NaN x, y (with -0.0 < +0.0).  The map is an involution.
 // ---------------------------------------------------------------------------------------------
