@@ -85,6 +85,39 @@ static int32_t launch_agg(const qdb_gb* gb, const AggArgs& a, int32_t ptype, boo
     }
 }
 
+static int32_t launch_spill(const qdb_gb* gb, const AggArgs& a, size_t smem, int64_t grid, cudaStream_t st) {
+    switch (val_kind(gb->val_type)) {
+        case VK_NONE:
+        case VK_I32: return launch_spill_t<int32_t>(a, smem, grid, st);
+        case VK_I64: return launch_spill_t<int64_t>(a, smem, grid, st);
+        case VK_F32: return launch_spill_t<float>(a, smem, grid, st);
+        case VK_F64: return launch_spill_t<double>(a, smem, grid, st);
+        default: return fail(QDB_ERR_INVALID, "unsupported value type");
+    }
+}
+
+// The table's spill area (kept across calls, grown on demand): rows key words, rows values of vbytes bytes,
+// and the fill counts of `cells` cells.
+static int32_t gb_spill_reserve(qdb_gb* gb, uint64_t rows, int vbytes, int64_t cells, cudaStream_t s) {
+    if (gb->spill_rows >= rows && gb->spill_vbytes >= vbytes && gb->spill_cells >= cells) return QDB_OK;
+    dev_free(gb->spill_keys, s);
+    dev_free(gb->spill_vals, s);
+    dev_free(gb->spill_fill, s);
+    gb->spill_keys = nullptr;
+    gb->spill_vals = nullptr;
+    gb->spill_fill = nullptr;
+    gb->spill_rows = 0;
+    gb->spill_cells = 0;
+    int32_t rc = dev_alloc(reinterpret_cast<void**>(&gb->spill_fill), static_cast<size_t>(cells) * sizeof(uint32_t), s);
+    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&gb->spill_keys), rows * 8, s);
+    if (rc == QDB_OK && vbytes) rc = dev_alloc(&gb->spill_vals, rows * static_cast<uint64_t>(vbytes), s);
+    if (rc != QDB_OK) return rc;
+    gb->spill_rows = rows;
+    gb->spill_vbytes = vbytes;
+    gb->spill_cells = cells;
+    return QDB_OK;
+}
+
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 static int64_t env_int(const char* name, int64_t dflt) {
@@ -269,6 +302,9 @@ int32_t qdb_gb_destroy(qdb_gb* gb) {
     dev_free(gb->main.slots, 0);
     dev_free(gb->aux.slots, 0);
     dev_free(gb->counters, 0);
+    dev_free(gb->spill_keys, 0);
+    dev_free(gb->spill_vals, 0);
+    dev_free(gb->spill_fill, 0);
     if (prev != gb->device) cudaSetDevice(prev);
     delete gb;
     return QDB_OK;
@@ -353,11 +389,16 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     a.capacity = static_cast<unsigned long long>(gb->capacity);
     const bool nulls = a.knull0 || a.knull1 || a.vnull || a.pnull;
 
-    // Tile and stage plan.
+    // Tile and stage plan: stages of about 32 KB (a stage costs a fixed hand-off between the producer and
+    // the consumers, so small stages cannot reach the HBM bandwidth), three of them in the ring.
     const DeviceInfo& di = device_info();
     const int ks = (gb->n_key_cols == 2) ? 4 : type_size(gb->key_type);
-    int Rw = static_cast<int>(env_int("QDB_AGG_ROWS_PER_WARP", 64));
-    Rw = std::max(kRowsPerWarpUnit, (Rw / kRowsPerWarpUnit) * kRowsPerWarpUnit);
+    int row_bytes = ks * gb->n_key_cols + (a.vals ? type_size(gb->val_type) : 0) + (a.pcol ? type_size(pred->type) : 0) +
+                    (a.mask ? 1 : 0);
+    if (row_bytes < 1) row_bytes = 1;
+    int Rw = static_cast<int>(env_int("QDB_AGG_ROWS_PER_WARP",
+                                      (32 * 1024) / (row_bytes * kConsumerWarps)));
+    Rw = std::min(512, std::max(kRowsPerWarpUnit, (Rw / kRowsPerWarpUnit) * kRowsPerWarpUnit));
     int T = kConsumerWarps * Rw;
     auto col_bytes = [&](int rows, int elem) { return static_cast<int32_t>(((size_t)rows * elem + 127) & ~size_t(127)); };
     auto plan_stage = [&](int rows) {
@@ -397,45 +438,101 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     const size_t bar_bytes = 128;
     const size_t list_bytes = (static_cast<size_t>(T) * 2 + 127) & ~size_t(127);
     const size_t queue_bytes = static_cast<size_t>(kConsumerWarps) * kQueueCap * (8 + 8 + 4);
-    const size_t budget =
-        static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes - queue_bytes;
 
-    // Shared-memory hash table sizing.
+    // Shared-memory table: bytes per slot (key, count, sum limbs, min/max).
+    const bool has_mm = a.has_min || a.has_max;
+    const bool vfloat = vk == VK_F32 || vk == VK_F64;
+    const size_t limb_bytes = a.has_sum ? (vfloat ? 12 : 8) : 0;
+    const size_t mm_bytes = has_mm ? (vk_is_32(vk) ? 8 : 16) : 0;
+    const size_t bps = 8 + 4 + limb_bytes + mm_bytes;
+    auto layout_table = [&](AggArgs& x, int S) {  // offsets of the table arrays; returns the bytes used
+        const size_t S2 = static_cast<size_t>(S) + 2;
+        size_t off = S2 * 8;
+        x.so_mn = static_cast<int32_t>(off); off += S2 * mm_bytes;
+        x.so_cnt = static_cast<int32_t>(off); off += S2 * 4;
+        x.so_l0 = static_cast<int32_t>(off); off += a.has_sum ? S2 * 4 : 0;
+        x.so_l1 = static_cast<int32_t>(off); off += a.has_sum ? S2 * 4 : 0;
+        x.so_l2 = static_cast<int32_t>(off); off += (a.has_sum && vfloat) ? S2 * 4 : 0;
+        return (off + 127) & ~size_t(127);
+    };
+
+    // Spill plan: when the table's group bound does not fit the shared table, misses are partitioned by key
+    // hash into 2^bits partitions, each small enough for the spill pass's shared table.
+    const bool smem_place = gb->placement != QDB_PLACE_GLOBAL;
+    int spill_bits = -1;
+    int S2spill = 0;
+    if (smem_place && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
+        const size_t budget2 = 100 * 1024;  // two spill-pass CTAs per SM
+        int S2 = 1 << 15;
+        while (S2 >= 256 && static_cast<size_t>(S2 + 2) * bps + 256 > budget2) S2 >>= 1;
+        if (S2 >= 256) {
+            const uint64_t per = static_cast<uint64_t>(S2) / 2;  // distinct keys per partition at load factor 1/2
+            const uint64_t parts = next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per);
+            int bits = 0;
+            while ((1ull << bits) < parts) ++bits;
+            if (bits <= 10) {
+                spill_bits = bits;
+                S2spill = S2;
+            }
+        }
+    }
+    const size_t spill_words_bytes = spill_bits >= 0 ? ((size_t(4) << spill_bits) + 127) & ~size_t(127) : 0;
+    const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes -
+                          queue_bytes - spill_words_bytes;
+
     size_t hash_bytes = 0;
-    if (gb->placement != QDB_PLACE_GLOBAL) {
-        const bool has_mm = a.has_min || a.has_max;
-        const size_t bps = 8 + 4 + (a.has_sum ? 8 : 0) + (has_mm ? (vk_is_32(vk) ? 8 : 16) : 0);
+    if (smem_place) {
         int S = 1 << 16;
-        while (S >= 256 && static_cast<size_t>(S + 2) * bps + 64 > budget) S >>= 1;
+        while (S >= 256 && static_cast<size_t>(S + 2) * bps + 128 > budget) S >>= 1;
         // A table much larger than the group count only costs initialisation and merge time.
         const uint64_t want = next_pow2(static_cast<uint64_t>(gb->capacity) * 2 + 2);
         if (static_cast<uint64_t>(S) > want) S = static_cast<int>(std::max<uint64_t>(want, 256));
         const int64_t forced = env_int("QDB_AGG_SMEM_SLOTS", 0);
         if (forced > 0 && forced < S) S = static_cast<int>(next_pow2(static_cast<uint64_t>(forced)));
         if (S >= 256) {
-            const size_t S2 = S + 2;
             a.S = S;
-            a.probe = (static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2)
-                          ? S : static_cast<int>(env_int("QDB_AGG_PROBE", 4));
-            size_t off = S2 * 8;
-            if (a.has_sum) { a.so_sum = static_cast<int32_t>(off); off += S2 * 8; }
-            if (has_mm) {
-                a.so_mn = static_cast<int32_t>(off);
-                off += S2 * 8;
-                if (vk_is_32(vk)) a.so_mx = a.so_mn;
-                else { a.so_mx = static_cast<int32_t>(off); off += S2 * 8; }
-            }
-            a.so_cnt = static_cast<int32_t>(off);
-            off += S2 * 4;
-            hash_bytes = (off + 127) & ~size_t(127);
+            const bool fits = static_cast<uint64_t>(gb->capacity) + 2 <= static_cast<uint64_t>(S) / 2;
+            a.probe = fits ? S : static_cast<int>(env_int("QDB_AGG_PROBE", 4));
+            hash_bytes = layout_table(a, S);
+            if (fits) spill_bits = -1;  // every group fits the shared table: no misses to spill
+        } else {
+            spill_bits = -1;
         }
+    }
+    if (spill_bits >= 0) {
+        // Spill area: one cell per (partition, CTA).  A cell holds 5/4 of its share of this call's rows (at most
+        // 2^27) plus 64, so hashed misses overflow a cell only when nearly every row misses the shared table.
+        const int64_t parts = int64_t(1) << spill_bits;
+        const int64_t ctas = std::min<int64_t>(di.sm_count, a.tiles);
+        const int64_t rows = std::min<int64_t>(n, int64_t(1) << 27);
+        const int64_t cell = (rows + rows / 4) / (parts * ctas) + 64;
+        const int vbytes = a.vals ? type_size(gb->val_type) : 0;
+        int32_t rc = gb_spill_reserve(gb, static_cast<uint64_t>(parts * ctas * cell), vbytes, parts * ctas, s);
+        if (rc != QDB_OK) return rc;
+        a.spill_keys = gb->spill_keys;
+        a.spill_vals = vbytes ? gb->spill_vals : nullptr;
+        a.spill_fill = gb->spill_fill;
+        a.spill_cell = cell;
+        a.spill_bits = spill_bits;
+        a.spill_ctas = static_cast<int32_t>(ctas);
     }
     a.so_bar = static_cast<int32_t>(hash_bytes);
     a.so_list = static_cast<int32_t>(hash_bytes + bar_bytes);
     a.so_queue = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes);
-    a.so_stage = static_cast<int32_t>(hash_bytes + bar_bytes + list_bytes + ((queue_bytes + 127) & ~size_t(127)));
+    a.so_spill = static_cast<int32_t>(a.so_queue + ((queue_bytes + 127) & ~size_t(127)));
+    a.so_stage = static_cast<int32_t>(a.so_spill + spill_words_bytes);
     const size_t smem = a.so_stage + stage_area;
-    return launch_agg(gb, a, ptype, nulls, smem, s);
+    int32_t rc = launch_agg(gb, a, ptype, nulls, smem, s);
+    if (rc != QDB_OK || spill_bits < 0) return rc;
+
+    // Spill pass: partitions x slices CTAs, each with a shared table of S2spill slots.
+    AggArgs b = a;
+    b.S = S2spill;
+    b.probe = 64;
+    const size_t smem2 = layout_table(b, S2spill);
+    const int64_t parts = int64_t(1) << spill_bits;
+    const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, (2 * di.sm_count + parts - 1) / parts));
+    return launch_spill(gb, b, smem2, parts * slices, s);
 }
 
 

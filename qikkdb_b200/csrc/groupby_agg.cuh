@@ -6,18 +6,21 @@
 //   * a producer warp streams the CTA's tiles of every input column (keys, values, predicate column,
 //     mask, null words) from HBM into a ring of shared-memory stages with bulk asynchronous copies
 //     (cp.async.bulk, executed by the TMA engine) that complete on per-stage mbarriers;
-//   * 30 consumer warps take the stages in order.  For every row they evaluate the predicate as an
+//   * 16 consumer warps take the stages in order.  For every row they evaluate the predicate as an
 //     interval test in the column's own type (the host turns `col OP constant` into [lo, hi] plus an
-//     invert flag, so the test is two compares and no branch), read the key, and insert it
-//       - first into a per-CTA shared-memory table (bounded linear probe, shared-memory atomics), which
-//         absorbs low-cardinality and skewed (Zipf) key streams,
-//       - on a miss, into the global open-addressing table (bounded linear probe, 64-bit atomicCAS on the
-//         key word, fire-and-forget reductions on the state words).  Misses are queued per warp and
-//         inserted 32 at a time with every lane active, so 32 probe loads of a warp are in flight together;
-//     then release the stage to the producer.  No mask or compacted column is written to HBM.
-// A warp that sees a low shared-memory hit rate after its first tiles stops probing shared memory.
+//     invert flag, so the test is two compares and no branch), compact the passing rows per warp, read
+//     the key, and insert it into a per-CTA shared-memory table (bounded linear probe) whose state is
+//     updated with 32-bit shared-memory atomics only (exact multi-limb sums), so skewed (Zipf) key
+//     streams do not serialise on hot slots.  A row whose key misses the table goes
+//       - to a hash-partitioned spill area in HBM when the table's group bound is larger than the
+//         shared table (gb_spill_kernel aggregates each partition in shared memory afterwards), or
+//       - to the global open-addressing table (bounded linear probe, 64-bit atomicCAS on the key word,
+//         fire-and-forget reductions), queued per warp and inserted 32 at a time after the stage has
+//         been released;
+//     no mask or compacted column is written to HBM.
 // At the end each CTA merges its shared-memory table into the global table.
-// Every wait on an mbarrier is bounded; a wait that gives up records QDB_ERR_TIMEOUT in the table status.
+// Every wait on an mbarrier or a spill chunk is bounded; an mbarrier wait that gives up records
+// QDB_ERR_TIMEOUT in the table status, a chunk wait that gives up sends its row to the global table.
 #pragma once
 
 #include <climits>
@@ -26,11 +29,12 @@
 
 namespace qdb {
 
-constexpr int kConsumerWarps = 30;
-constexpr int kConsumerThreads = kConsumerWarps * 32;     // 960
-constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer warp: 992 threads
+constexpr int kConsumerWarps = 16;
+constexpr int kConsumerThreads = kConsumerWarps * 32;     // 512
+constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer warp: 544 threads
 constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsumerWarps * R rows, R a multiple of 64
-constexpr int kQueueCap = 64;                              // per-warp queue of shared-memory misses
+constexpr int kQueueCap = 64;                              // per-warp queue of rows for the global table
+constexpr int kSpillThreads = 512;                         // threads of a spill-pass CTA
 constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
 constexpr uint32_t kMaxWaitIters = 1u << 24;               // bounded mbarrier waits (seconds, then give up)
 
@@ -60,7 +64,7 @@ struct AggArgs {
     PredInterval pi;
     const int8_t* mask = nullptr;
     int64_t n = 0;
-    int32_t T = 1920;        // rows per tile: kConsumerWarps * R with R a multiple of 64
+    int32_t T = 2048;        // rows per tile: kConsumerWarps * R with R a multiple of 64
     int32_t NS = 3;          // stages in the ring
     int64_t tiles = 0;       // all tiles, the last one possibly partial
     int64_t full_tiles = 0;  // tiles with T rows
@@ -77,8 +81,17 @@ struct AggArgs {
     int32_t S = 0;       // shared-memory hash slots (power of two) or 0 for a global-only pass
     int32_t probe = 0;   // shared-memory probe limit
     // byte offsets inside dynamic shared memory
-    int32_t so_stage = 0, so_bar = 0, so_list = 0, so_queue = 0;
-    int32_t so_sum = 0, so_mn = 0, so_mx = 0, so_cnt = 0;  // hash arrays (keys at offset 0), S + 2 entries each
+    int32_t so_stage = 0, so_bar = 0, so_list = 0, so_queue = 0, so_spill = 0;
+    // shared table arrays (keys at offset 0, S + 2 entries each): counts, sum limbs, min/max
+    int32_t so_cnt = 0, so_l0 = 0, so_l1 = 0, so_l2 = 0, so_mn = 0;
+    // hash-partitioned spill of shared-table misses (spill_keys == nullptr: misses go to the global table).
+    // Cell (c, p), the rows CTA c spills into partition p, holds spill_cell rows at (p * spill_ctas + c) * spill_cell.
+    uint64_t* spill_keys = nullptr;  // key words
+    void* spill_vals = nullptr;      // values (absent without a value column)
+    uint32_t* spill_fill = nullptr;  // [partitions * spill_ctas] rows written per cell
+    int64_t spill_cell = 0;          // rows per cell
+    int32_t spill_bits = 0;          // log2 of the partition count
+    int32_t spill_ctas = 0;          // CTAs of the aggregation pass (its grid)
 };
 
 template <typename A, typename B>
@@ -322,6 +335,92 @@ __device__ __forceinline__ uint32_t smem_hash(uint64_t kw, int shift) {
     return (f * 0x9e3779b1u) >> shift;
 }
 
+// Shared-memory accesses by 32-bit shared-window address (PTX ld/atom/red .shared), so the table code does its
+// address arithmetic in 32 bits.  Keys are never removed from a table, so a weak read of a key word can only be
+// stale by showing an empty slot, which the claiming CAS then corrects.
+__device__ __forceinline__ uint64_t lds64(uint32_t a) {
+    uint64_t v;
+    asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ int32_t lds32(uint32_t a) {
+    int32_t v;
+    asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ int64_t lds64s(uint32_t a) {
+    int64_t v;
+    asm volatile("ld.shared.s64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atoms_add(uint32_t a, unsigned x) {
+    unsigned old;
+    asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(x) : "memory");
+    return old;
+}
+__device__ __forceinline__ void reds_add(uint32_t a, unsigned x) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a), "r"(x) : "memory");
+}
+__device__ __forceinline__ void reds_min32(uint32_t a, int32_t x) {
+    asm volatile("red.shared.min.s32 [%0], %1;" ::"r"(a), "r"(x) : "memory");
+}
+__device__ __forceinline__ void reds_max32(uint32_t a, int32_t x) {
+    asm volatile("red.shared.max.s32 [%0], %1;" ::"r"(a), "r"(x) : "memory");
+}
+__device__ __forceinline__ void reds_min64(uint32_t a, int64_t x) {
+    asm volatile("red.shared.min.s64 [%0], %1;" ::"r"(a), "l"(x) : "memory");
+}
+__device__ __forceinline__ void reds_max64(uint32_t a, int64_t x) {
+    asm volatile("red.shared.max.s64 [%0], %1;" ::"r"(a), "l"(x) : "memory");
+}
+__device__ __forceinline__ uint64_t atoms_cas64(uint32_t a, uint64_t cmp, uint64_t val) {
+    uint64_t old;
+    asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(a), "l"(cmp), "l"(val) : "memory");
+    return old;
+}
+
+// Shared-memory probe by address: table key words at `keys` (S slots, S a power of two), starting at slot h.
+// Returns the slot, or -1 after P probes; *found is set when the key was already present.
+__device__ __forceinline__ int s_find32(uint32_t keys, int S, int P, uint64_t key, uint32_t h, bool* found) {
+    uint32_t s = h;
+    for (int p = 0; p < P; ++p) {
+        const uint64_t cur = lds64(keys + s * 8u);
+        if (cur == key) {
+            *found = true;
+            return static_cast<int>(s);
+        }
+        if (cur == kEmpty) {
+            const uint64_t prev = atoms_cas64(keys + s * 8u, kEmpty, key);
+            if (prev == kEmpty) return static_cast<int>(s);
+            if (prev == key) {
+                *found = true;
+                return static_cast<int>(s);
+            }
+        }
+        s = (s + 1u) & static_cast<uint32_t>(S - 1);
+    }
+    return -1;
+}
+
+// The table is read as 4-way buckets: a key's home is slot 4 * bucket, and a bounded linear probe that starts
+// there (the generic path, and the claim of a new key) visits the bucket's four slots first.  The common case
+// reads the whole bucket with two 16-byte loads and compares the four key words without a loop.
+__device__ __forceinline__ uint32_t bucket_home(uint64_t kw, int smem_shift) { return smem_hash(kw, smem_shift + 2) * 4u; }
+
+// Returns the slot of kw in the bucket at slot h4 (or -1); *has_empty tells whether the bucket has a free slot.
+__device__ __forceinline__ int probe4(uint32_t keys, uint32_t h4, uint64_t kw, bool* has_empty) {
+    uint4 w0, w1;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(w0.x), "=r"(w0.y), "=r"(w0.z), "=r"(w0.w) : "r"(keys + h4 * 8u) : "memory");
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(w1.x), "=r"(w1.y), "=r"(w1.z), "=r"(w1.w) : "r"(keys + h4 * 8u + 16u) : "memory");
+    const uint64_t k0 = (static_cast<uint64_t>(w0.y) << 32) | w0.x, k1 = (static_cast<uint64_t>(w0.w) << 32) | w0.z;
+    const uint64_t k2 = (static_cast<uint64_t>(w1.y) << 32) | w1.x, k3 = (static_cast<uint64_t>(w1.w) << 32) | w1.z;
+    *has_empty = (k0 == kEmpty) | (k1 == kEmpty) | (k2 == kEmpty) | (k3 == kEmpty);
+    return (k0 == kw) ? static_cast<int>(h4) : (k1 == kw) ? static_cast<int>(h4 + 1) :
+           (k2 == kw) ? static_cast<int>(h4 + 2) : (k3 == kw) ? static_cast<int>(h4 + 3) : -1;
+}
+
 // Shared-memory probe.  Returns the slot, or -1 after `P` probes.  *found is set when the key was
 // already present (a reuse rather than a first claim).
 __device__ __forceinline__ int s_find(uint64_t* skey, int S, int P, uint64_t key, uint32_t h, bool* found) {
@@ -346,65 +445,240 @@ __device__ __forceinline__ int s_find(uint64_t* skey, int S, int P, uint64_t key
     return -1;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Shared-memory slot state.  Every update is a 32-bit shared-memory atomic: those are resolved by the
+// shared-memory atomic unit even when many lanes and warps hit one address (a skewed key stream), while
+// 64-bit shared-memory atomics (CAS loops) serialise on hot slots.
+//   count : u32 per slot (the rows one CTA adds to one slot fit 32 bits).
+//   sum   : integer values: a 64-bit two's-complement accumulator kept as two u32 limbs; the carry out of
+//           the low limb is detected from the value the atomic returns and added to the high limb, so the
+//           sum is exact and wraps like the reference's 64-bit integer atomicAdd.
+//           float/double values: a 96-bit fixed-point accumulator (three u32 limbs) of q = round(v * 2^F),
+//           F chosen per CTA from the magnitudes of its first tile (fix_scale).  Values outside the window
+//           where q keeps at least 24 significant bits and |q| < 2^63 (and NaN/Inf) take the global FP64 path.
+//   min/max : order-preserving encodings; 32-bit atomics for 32-bit values, 64-bit ones for 64-bit values,
+//           both issued only when the value improves on the slot's current bound.
+// ---------------------------------------------------------------------------------------------
+struct FixScale {
+    double scale = 1.0;  // 2^F
+    double inv = 1.0;    // 2^-F
+    double lo = 0.0;     // smallest magnitude kept in fixed point
+    double hi = 0.0;     // magnitudes at or above this take the FP64 path
+    int sh0 = 0;         // float values: q = mantissa << (biased exponent - sh0), kept when 1 <= shift <= 39
+};
+
+// emax: the largest binary exponent e (|v| < 2^e) seen in the CTA's first tile.
+__device__ __forceinline__ FixScale fix_scale(int emax) {
+    emax = max(-960, min(960, emax));
+    FixScale f;
+    f.scale = ldexp(1.0, 48 - emax);
+    f.inv = ldexp(1.0, emax - 48);
+    f.lo = ldexp(1.0, emax - 24);
+    f.hi = ldexp(1.0, emax + 15);
+    f.sh0 = emax + 102;
+    return f;
+}
+
+// Binary exponent e with |v| < 2^e for a finite non-zero value, INT_MIN otherwise.
 template <typename VT>
-__device__ __forceinline__ void s_acc_row(unsigned char* sm, const AggArgs& a, int s, VT v, bool has_val) {
-    atomicAdd(reinterpret_cast<unsigned int*>(sm + a.so_cnt) + s, 1u);
+__device__ __forceinline__ int value_exp(VT v) {
+    if constexpr (std::is_same<VT, float>::value) {
+        const uint32_t b = __float_as_uint(v);
+        const int e = static_cast<int>((b >> 23) & 0xffu);
+        return (e == 0 || e == 0xff) ? INT_MIN : e - 126;
+    } else if constexpr (std::is_same<VT, double>::value) {
+        const uint64_t b = static_cast<uint64_t>(__double_as_longlong(v));
+        const int e = static_cast<int>((b >> 52) & 0x7ffu);
+        return (e == 0 || e == 0x7ff) ? INT_MIN : e - 1022;
+    } else {
+        return INT_MIN;
+    }
+}
+
+// The fixed-point (or exact integer) addend of one value; ok is false when the value must take the FP64 path.
+template <typename VT>
+__device__ __forceinline__ long long sum_addend(VT v, const FixScale& f, bool* ok) {
+    if constexpr (std::is_same<VT, float>::value) {
+        // integer-only: v = +-m * 2^(e - 150) with m the 24-bit significand, so q = +-m << (e - sh0) exactly
+        const uint32_t b = __float_as_uint(v);
+        const int e = static_cast<int>((b >> 23) & 0xffu);
+        const uint32_t fr = b & 0x7fffffu;
+        if (e == 0) {
+            *ok = fr == 0u;  // zero is exact; subnormals take the FP64 path
+            return 0ll;
+        }
+        const int sh = e - f.sh0;
+        *ok = e != 0xff && sh >= 1 && sh <= 39;
+        const long long q = *ok ? static_cast<long long>(static_cast<uint64_t>(fr | 0x800000u) << sh) : 0ll;
+        return (b >> 31) ? -q : q;
+    } else if constexpr (std::is_floating_point<VT>::value) {
+        const double d = static_cast<double>(v);
+        const double m = fabs(d);
+        *ok = (m == 0.0) || (m >= f.lo && m < f.hi);  // false for NaN and Inf
+        return *ok ? __double2ll_rn(d * f.scale) : 0ll;
+    } else {
+        *ok = true;
+        return static_cast<long long>(v);
+    }
+}
+
+struct STable {
+    uint64_t* key;
+    unsigned* cnt;
+    unsigned* l0;
+    unsigned* l1;
+    unsigned* l2;
+    unsigned char* mm;  // min/max region
+    // the same arrays as 32-bit shared-window addresses
+    uint32_t ak, ac, a0, a1, a2, am;
+};
+
+__device__ __forceinline__ STable stable(unsigned char* sm, const AggArgs& a) {
+    STable t;
+    t.key = reinterpret_cast<uint64_t*>(sm);
+    t.cnt = reinterpret_cast<unsigned*>(sm + a.so_cnt);
+    t.l0 = reinterpret_cast<unsigned*>(sm + a.so_l0);
+    t.l1 = reinterpret_cast<unsigned*>(sm + a.so_l1);
+    t.l2 = reinterpret_cast<unsigned*>(sm + a.so_l2);
+    t.mm = sm + a.so_mn;
+    t.ak = smem_u32(t.key);
+    t.ac = smem_u32(t.cnt);
+    t.a0 = smem_u32(t.l0);
+    t.a1 = smem_u32(t.l1);
+    t.a2 = smem_u32(t.l2);
+    t.am = smem_u32(t.mm);
+    return t;
+}
+
+// Adds the sign-extended 64-bit addend q to slot s's limbs (2 limbs: 64-bit wrap; 3 limbs: 96-bit).
+template <int LIMBS>
+__device__ __forceinline__ void limbs_add(const STable& t, int s, long long q) {
+    const unsigned long long uq = static_cast<unsigned long long>(q);
+    const unsigned x0 = static_cast<unsigned>(uq);
+    const unsigned x1 = static_cast<unsigned>(uq >> 32);
+    const uint32_t o = static_cast<uint32_t>(s) * 4u;
+    const unsigned old0 = atoms_add(t.a0 + o, x0);
+    const unsigned c = (old0 + x0 < old0) ? 1u : 0u;
+    if constexpr (LIMBS == 2) {
+        reds_add(t.a1 + o, x1 + c);  // the top limb wraps: the sum is exact modulo 2^64
+    } else {
+        const unsigned long long y1 = static_cast<unsigned long long>(x1) + c;
+        const unsigned y1l = static_cast<unsigned>(y1);
+        const unsigned old1 = atoms_add(t.a1 + o, y1l);
+        const unsigned c1 = static_cast<unsigned>(y1 >> 32) + ((old1 + y1l < old1) ? 1u : 0u);
+        const unsigned y2 = (q < 0 ? 0xffffffffu : 0u) + c1;
+        if (y2) reds_add(t.a2 + o, y2);
+    }
+}
+
+// The 96-bit fixed-point accumulator of a slot as a double (before scaling): |error| <= 2 ulp.
+__device__ __forceinline__ double limbs96_to_double(unsigned l0, unsigned l1, unsigned l2) {
+    unsigned long long lo = (static_cast<unsigned long long>(l1) << 32) | l0;
+    unsigned hi = l2;
+    const bool neg = (hi & 0x80000000u) != 0;
+    if (neg) {  // two's-complement negation of the 96-bit value
+        lo = ~lo + 1ull;
+        hi = ~hi + (lo == 0ull ? 1u : 0u);
+    }
+    const double m = static_cast<double>(hi) * 18446744073709551616.0 + static_cast<double>(lo);
+    return neg ? -m : m;
+}
+
+// One row's value into shared slot s (q: the precomputed sum addend).
+template <typename VT>
+__device__ __forceinline__ void s_add(const STable& t, const AggArgs& a, int s, VT v, long long q, bool has_val) {
+    reds_add(t.ac + static_cast<uint32_t>(s) * 4u, 1u);
     if (!has_val) return;
     if (a.has_sum) {
-        if constexpr (std::is_floating_point<VT>::value)
-            atomicAdd(reinterpret_cast<double*>(sm + a.so_sum) + s, static_cast<double>(v));
-        else
-            atomicAdd(reinterpret_cast<unsigned long long*>(sm + a.so_sum) + s,
-                      static_cast<unsigned long long>(static_cast<long long>(v)));
+        if constexpr (std::is_floating_point<VT>::value) limbs_add<3>(t, s, q);
+        else limbs_add<2>(t, s, q);
     }
-    if constexpr (sizeof(VT) == 4) {
-        const int32_t e = enc32(v);
-        if (a.has_min) atomicMin(reinterpret_cast<int*>(sm + a.so_mn) + 2 * s, e);
-        if (a.has_max) atomicMax(reinterpret_cast<int*>(sm + a.so_mx) + 2 * s + 1, e);
-    } else {
-        const long long e = enc64(v);
-        if (a.has_min) atomicMin(reinterpret_cast<long long*>(sm + a.so_mn) + s, e);
-        if (a.has_max) atomicMax(reinterpret_cast<long long*>(sm + a.so_mx) + s, e);
-    }
-}
-
-// Register accumulation helpers: the running sum of a group of rows (FP64 for float values, wrapping int64 for
-// integer values) and the order-preserving MIN/MAX encoding.
-template <typename VT>
-using AccOf = typename std::conditional<std::is_floating_point<VT>::value, double, long long>::type;
-
-template <typename VT>
-__device__ __forceinline__ AccOf<VT> to_acc(VT v) {
-    return static_cast<AccOf<VT>>(v);
-}
-
-template <typename VT>
-__device__ __forceinline__ long long enc_any(VT v) {
-    if constexpr (sizeof(VT) == 4) return enc32(v);
-    else return enc64(v);
-}
-
-// Merges c rows with sum `acc` and encoded min/max into shared slot s.
-template <typename VT>
-__device__ __forceinline__ void s_merge_acc(unsigned char* sm, const AggArgs& a, int s, unsigned c, AccOf<VT> acc,
-                                            long long mn, long long mx, bool has_val) {
-    atomicAdd(reinterpret_cast<unsigned int*>(sm + a.so_cnt) + s, c);
-    if (!has_val) return;
-    if (a.has_sum) {
-        if constexpr (std::is_floating_point<VT>::value)
-            atomicAdd(reinterpret_cast<double*>(sm + a.so_sum) + s, acc);
-        else
-            atomicAdd(reinterpret_cast<unsigned long long*>(sm + a.so_sum) + s, static_cast<unsigned long long>(acc));
-    }
-    if constexpr (sizeof(VT) == 4) {
-        if (a.has_min) atomicMin(reinterpret_cast<int*>(sm + a.so_mn) + 2 * s, static_cast<int>(mn));
-        if (a.has_max) atomicMax(reinterpret_cast<int*>(sm + a.so_mx) + 2 * s + 1, static_cast<int>(mx));
-    } else {
-        if (a.has_min) atomicMin(reinterpret_cast<long long*>(sm + a.so_mn) + s, mn);
-        if (a.has_max) atomicMax(reinterpret_cast<long long*>(sm + a.so_mx) + s, mx);
+    if (a.has_min || a.has_max) {
+        if constexpr (sizeof(VT) == 4) {
+            const int32_t e = enc32(v);
+            const uint32_t w = t.am + static_cast<uint32_t>(s) * 8u;
+            if (a.has_min && e < lds32(w)) reds_min32(w, e);
+            if (a.has_max && e > lds32(w + 4u)) reds_max32(w + 4u, e);
+        } else {
+            const long long e = enc64(v);
+            const uint32_t w = t.am + static_cast<uint32_t>(s) * 16u;
+            if (a.has_min && e < lds64s(w)) reds_min64(w, e);
+            if (a.has_max && e > lds64s(w + 8u)) reds_max64(w + 8u, e);
+        }
     }
 }
 
+// Initialises S2 slots of a shared table.
+template <typename VT>
+__device__ __forceinline__ void s_init(const STable& t, const AggArgs& a, int S2) {
+    const bool has_mm = a.has_min || a.has_max;
+    for (int i = threadIdx.x; i < S2; i += blockDim.x) {
+        t.key[i] = kEmpty;
+        t.cnt[i] = 0u;
+        if (a.has_sum) {
+            t.l0[i] = 0u;
+            t.l1[i] = 0u;
+            if (std::is_floating_point<VT>::value) t.l2[i] = 0u;
+        }
+        if (has_mm) {
+            if (sizeof(VT) == 4) {
+                reinterpret_cast<unsigned long long*>(t.mm)[i] = kPackedMinMaxInit;
+            } else {
+                reinterpret_cast<unsigned long long*>(t.mm)[2 * i] = kMinInit64;
+                reinterpret_cast<unsigned long long*>(t.mm)[2 * i + 1] = kMaxInit64;
+            }
+        }
+    }
+}
+
+// Merges every occupied slot of a shared table into the global table (whole CTA).
+template <typename VT>
+__device__ __forceinline__ void s_flush(const STable& t, const AggArgs& a, int S, const FixScale& fs,
+                                        unsigned long long* claims) {
+    const bool has_mm = a.has_min || a.has_max;
+    const bool v32 = sizeof(VT) == 4;
+    const bool vfloat = std::is_floating_point<VT>::value;
+    const int W = a.L.W;
+    for (int i = threadIdx.x; i < S + 2; i += blockDim.x) {
+        const uint64_t key = t.key[i];
+        if (key == kEmpty) continue;
+        uint64_t* slot = (i < S) ? g_find(a.main, W, key, mix64(key), a.counters, claims)
+                                 : g_special(a.main, W, i - S, claims);
+        if (!slot) continue;
+        const unsigned long long c = t.cnt[i];
+        uint64_t sumbits = 0;
+        if (a.has_sum) {
+            if (vfloat) {
+                const double d = limbs96_to_double(t.l0[i], t.l1[i], t.l2[i]) * fs.inv;
+                memcpy(&sumbits, &d, 8);
+            } else {
+                sumbits = (static_cast<uint64_t>(t.l1[i]) << 32) | t.l0[i];
+            }
+        }
+        long long mn = 0, mx = 0;
+        if (has_mm) {
+            if (v32) {
+                const int* w = reinterpret_cast<const int*>(t.mm) + 2 * i;
+                mn = w[0];
+                mx = w[1];
+            } else {
+                const long long* w = reinterpret_cast<const long long*>(t.mm) + 2 * i;
+                mn = w[0];
+                mx = w[1];
+            }
+        }
+        g_merge(slot, a.L, a.has_sum, a.has_min, a.has_max, v32, vfloat, c, sumbits, mn, mx);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Hash-partitioned spill of shared-memory misses.  A row whose key is not in the CTA's shared table is
+// appended to partition p = (top bits of its key hash) of a spill area in HBM instead of being inserted
+// into the global table with L2 atomics; gb_spill_kernel then aggregates each partition in shared memory
+// (a partition holds a bounded share of the distinct keys) and merges it into the global table.
+// Every CTA owns one cell of every partition, so an append is one 32-bit shared-memory atomic on the cell's
+// fill counter and two plain stores; a row that finds its cell full takes the global path instead.
+// ---------------------------------------------------------------------------------------------
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type
 // (int32_t when the table has no value column); PT: predicate column type or NoPred; NULLS: some null
@@ -414,33 +688,28 @@ template <typename KT, bool COMP, typename VT, typename PT, bool NULLS>
 __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ unsigned long long s_claims;
+    __shared__ int s_emax;
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
+    constexpr bool VFLOAT = std::is_floating_point<VT>::value;
+    constexpr bool FASTROW = !COMP && !NULLS;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
-    using AccT = AccOf<VT>;
 
     const int S = a.S;
-    const int S2 = S ? S + 2 : 0;
-    uint64_t* skey = reinterpret_cast<uint64_t*>(sm);
+    const STable tab = stable(sm, a);
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(sm + a.so_bar);
     uint64_t* empty_bar = full_bar + a.NS;
-    const bool has_mm = a.has_min || a.has_max;
+    unsigned* sfill = reinterpret_cast<unsigned*>(sm + a.so_spill);
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const bool spill_on = a.spill_keys != nullptr;
 
-    for (int i = threadIdx.x; i < S2; i += blockDim.x) {
-        skey[i] = kEmpty;
-        reinterpret_cast<unsigned int*>(sm + a.so_cnt)[i] = 0u;
-        if (a.has_sum) reinterpret_cast<unsigned long long*>(sm + a.so_sum)[i] = 0ull;
-        if (has_mm) {
-            if (sizeof(VT) == 4) {
-                reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kPackedMinMaxInit;
-            } else {
-                reinterpret_cast<unsigned long long*>(sm + a.so_mn)[i] = kMinInit64;
-                reinterpret_cast<unsigned long long*>(sm + a.so_mx)[i] = kMaxInit64;
-            }
-        }
+    if (S) s_init<VT>(tab, a, S + 2);
+    if (spill_on)
+        for (int i = threadIdx.x; i < (1 << a.spill_bits); i += blockDim.x) sfill[i] = 0u;
+    if (threadIdx.x == 0) {
+        s_claims = 0;
+        s_emax = INT_MIN;
     }
-    if (threadIdx.x == 0) s_claims = 0;
     if (threadIdx.x == 0 && a.staged) {
         for (int s = 0; s < a.NS; ++s) {
             mbar_init(&full_bar[s], 1);
@@ -454,6 +723,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         (a.tiles > static_cast<int64_t>(blockIdx.x)) ? (a.tiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
     const int W = a.L.W;
     const int T = a.T;
+    FixScale fs;
 
     if (warp == kConsumerWarps) {
         // ---------------- producer warp: one elected lane issues the bulk copies ----------------
@@ -461,12 +731,12 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             const StageLayout& sl = a.sl;
             const uint64_t pol = l2_evict_first_policy();
             int64_t q = 0;
+            int s = 0;
+            uint32_t ph = 0;  // phase of stage s's current round
             for (; q < my_tiles; ++q) {
                 const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
                 if (tile >= a.full_tiles) break;  // the partial last tile is read directly
-                const int s = static_cast<int>(q % a.NS);
-                if (q >= a.NS && !mbar_wait(&empty_bar[s], static_cast<uint32_t>((q / a.NS - 1) & 1), a.counters))
-                    break;
+                if (q >= a.NS && !mbar_wait(&empty_bar[s], ph ^ 1u, a.counters)) break;
                 unsigned char* st = sm + a.so_stage + static_cast<size_t>(s) * sl.bytes;
                 const int64_t r0 = tile * T;
                 const uint32_t words = static_cast<uint32_t>(T / 64) * 8u;
@@ -486,6 +756,10 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 if (sl.knull1 >= 0) bulk_g2s(st + sl.knull1, a.knull1 + r0 / 64, words, &full_bar[s], pol);
                 if (sl.vnull >= 0) bulk_g2s(st + sl.vnull, a.vnull + r0 / 64, words, &full_bar[s], pol);
                 if (sl.pnull >= 0) bulk_g2s(st + sl.pnull, a.pnull + r0 / 64, words, &full_bar[s], pol);
+                if (++s == a.NS) {
+                    s = 0;
+                    ph ^= 1u;
+                }
             }
             // Drain: every issued stage must have been consumed (so no copy is still in flight) before exit.
             for (int64_t d = (q > a.NS ? q - a.NS : 0); d < q; ++d) {
@@ -502,296 +776,475 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         const PL plo = HAS_PRED ? from_bits<PL>(a.pi.lo) : PL{};
         const PL phi = HAS_PRED ? from_bits<PL>(a.pi.hi) : PL{};
         const bool pinv = a.pi.invert != 0;
-        bool use_smem = S > 0;
-        unsigned my_hits = 0, my_tries = 0;
         const int R = T / kConsumerWarps;
         uint16_t* list = reinterpret_cast<uint16_t*>(sm + a.so_list) + warp * R;
         const uint32_t lt_mask = (1u << lane) - 1u;
+
+        // Fixed-point scale of float sums: the largest exponent of this CTA's first tile of values.
+        if (VFLOAT && a.has_sum && has_vals && my_tiles > 0) {
+            const int64_t tile = blockIdx.x;
+            const bool staged = a.staged && tile < a.full_tiles;
+            bool ok = true;
+            if (staged) ok = mbar_wait(&full_bar[0], 0u, a.counters);
+            int e = INT_MIN;
+            if (ok) {
+                const unsigned char* st = sm + a.so_stage;
+                for (int j = lane; j < R; j += 32) {
+                    const int i = warp * R + j;
+                    const int64_t r = tile * T + i;
+                    if (r < a.n) {
+                        const VT v = staged ? reinterpret_cast<const VT*>(st + a.sl.val)[i] : static_cast<const VT*>(a.vals)[r];
+                        e = max(e, value_exp<VT>(v));
+                    }
+                }
+            }
+            e = __reduce_max_sync(0xffffffffu, e);
+            if (lane == 0 && e != INT_MIN) atomicMax(&s_emax, e);
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kConsumerThreads) : "memory");
+        fs = fix_scale(s_emax == INT_MIN ? 0 : s_emax);
+
+        bool use_smem = S > 0;
+        unsigned my_hits = 0, my_tries = 0;
         const int smem_shift = 32 - (31 - __clz(S > 0 ? S : 1));
-        // Per-warp queue of shared-memory misses (raw rows: key word, value bits, kind | agg flag).
+        // Per-warp queue of rows for the global table (raw rows: key word, value bits, kind | agg flag).
         uint64_t* qkw = reinterpret_cast<uint64_t*>(sm + a.so_queue) + warp * kQueueCap;
         uint64_t* qval = reinterpret_cast<uint64_t*>(sm + a.so_queue) + (kConsumerWarps + warp) * kQueueCap;
         uint32_t* qmeta = reinterpret_cast<uint32_t*>(reinterpret_cast<uint64_t*>(sm + a.so_queue) +
                                                       2 * kConsumerWarps * kQueueCap) + warp * kQueueCap;
         int qn = 0;
-        // Two hot keys per warp (the CTA's most frequent shared slots after the first tiles) with per-lane
-        // register accumulators.  64-bit shared atomics serialise when many warps update one slot, so a skewed
-        // key stream would otherwise queue on its hottest slots.
-        uint64_t hk0 = kEmpty, hk1 = kEmpty;  // kEmpty never equals a NORMAL key word
-        unsigned hc0 = 0, hc1 = 0;
-        AccT ha0 = AccT{}, ha1 = AccT{};
-        long long hmn0 = LLONG_MAX, hmx0 = LLONG_MIN, hmn1 = LLONG_MAX, hmx1 = LLONG_MIN;
-        auto pick_hot_keys = [&]() {
-            // warp-wide argmax of the shared slot counts, twice; only keys with a real share of the rows
-            const unsigned* cnt = reinterpret_cast<const unsigned*>(sm + a.so_cnt);
-            unsigned total = 0, b0 = 0, b1 = 0;
-            for (int i = lane; i < S; i += 32) {
-                const unsigned c = cnt[i];
-                total += c;
-                const unsigned key = (min(c, 0x7ffffu) << 13) | static_cast<unsigned>(i & 0x1fff);
-                if (key > b0) {
-                    b1 = b0;
-                    b0 = key;
-                } else if (key > b1) {
-                    b1 = key;
-                }
-            }
-            total = __reduce_add_sync(0xffffffffu, total);
-            const unsigned w0 = __reduce_max_sync(0xffffffffu, b0);
-            const unsigned c0 = (b0 == w0) ? b1 : b0;  // the owner of the first pick offers its runner-up
-            const unsigned w1 = __reduce_max_sync(0xffffffffu, c0);
-            if (S <= 8192 && w0 && (w0 >> 13) * 32u >= total) hk0 = skey[w0 & 0x1fffu];
-            if (S <= 8192 && w1 && (w1 >> 13) * 32u >= total) hk1 = skey[w1 & 0x1fffu];
-            if (hk0 == kEmpty) hk1 = kEmpty;
-        };
-        // Reduces a hot key's per-lane partials over the warp and merges them into the key's shared slot.
-        auto flush_hot = [&](uint64_t hk, unsigned c, AccT acc, long long mn, long long mx) {
-            if (hk == kEmpty) return;
-            for (int o = 16; o > 0; o >>= 1) {
-                c += __shfl_xor_sync(0xffffffffu, c, o);
-                acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            }
-            if (lane == 0 && c) {
-                bool found = false;
-                const int s = s_find(skey, S, S, hk, smem_hash(hk, smem_shift), &found);
-                if (s >= 0) s_merge_acc<VT>(sm, a, s, c, acc, mn, mx, has_vals);
-            }
-        };
-        // Global inserts of queued misses: `issue` pops queue entry e into this lane's registers and issues the
-        // first probe load; `complete` finishes the probe and applies the reductions.  A whole warp drains 32
-        // entries at once, so 32 probe loads are in flight together.  (Deferring `complete` by one batch to
-        // overlap the round trip with the next tile measured slower.)
-        bool pf = false;
-        uint64_t pf_kw = 0, pf_val = 0, pf_word = 0, pf_s = 0;
-        uint32_t pf_meta = 0;
-        auto issue = [&](int e) {
-            pf_kw = qkw[e];
-            pf_val = qval[e];
-            pf_meta = qmeta[e];
-            pf = true;
-            const int kind = static_cast<int>(pf_meta & 3u);
-            if (kind == KK_NORMAL || kind == KK_AUX) {
-                const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
-                pf_s = mix64(pf_kw) & Rg.mask;
-                pf_word = ld_volatile_u64(Rg.slots + pf_s * W);
-            }
-        };
-        auto complete = [&]() {
-            if (!pf) return;
-            pf = false;
-            const int kind = static_cast<int>(pf_meta & 3u);
+        // Global inserts of queued rows, 32 at a time with every lane active, so the warp's 32 probe loads
+        // are in flight together.
+        auto drain32 = [&](int first) {
+            const int e = first + lane;
+            const uint64_t kw = qkw[e];
+            const uint64_t vb = qval[e];
+            const uint32_t meta = qmeta[e];
+            const int kind = static_cast<int>(meta & 3u);
             uint64_t* slot;
             if (kind == KK_NORMAL || kind == KK_AUX) {
                 const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
-                slot = g_find_from(Rg, W, pf_kw, pf_s, pf_word, a.counters, &s_claims);
+                slot = g_find(Rg, W, kw, mix64(kw), a.counters, &s_claims);
             } else {
                 slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, &s_claims);
             }
-            if (slot && (pf_meta & 4u)) {
+            if (slot && (meta & 4u)) {
                 if (has_vals) {
                     VT v;
-                    memcpy(&v, &pf_val, sizeof(VT));
+                    memcpy(&v, &vb, sizeof(VT));
                     g_acc_row<VT>(slot, a, v);
                 } else {
                     g_count_row(slot, a.L);
                 }
             }
         };
-        for (int64_t q = 0; q < my_tiles; ++q) {
-            const int64_t tile = blockIdx.x + q * static_cast<int64_t>(gridDim.x);
+        // Spill cell addressing of this CTA: row pos of partition p is at p * pstride + cell_off + pos.
+        const int64_t pstride = spill_on ? static_cast<int64_t>(a.spill_ctas) * a.spill_cell : 0;
+        const int64_t cell_off = spill_on ? static_cast<int64_t>(blockIdx.x) * a.spill_cell : 0;
+        const unsigned cell_cap = spill_on ? static_cast<unsigned>(a.spill_cell) : 0u;
+        VT* const spill_v = static_cast<VT*>(a.spill_vals);
+        const uint32_t sfill_a = smem_u32(sfill);
+        const int K = R >> 5;  // rows per lane in phase A
+        // One passing row (list entry e): probe the shared table, update the slot, or spill; returns true when the
+        // row must go to the warp's queue of global inserts.
+        auto insert_row = [&](int e, const unsigned char* st, bool staged, int64_t base, uint64_t& kw_out,
+                              VT& v_out, uint32_t& meta_out) -> bool {
+            const int i = list[e];
+            KT k0, k1 = KT{};
+            bool kn0 = false, kn1 = false, vn = false;
+            VT v = VT{};
+            if (staged) {
+                k0 = reinterpret_cast<const KT*>(st + a.sl.key0)[i];
+                if constexpr (COMP) k1 = reinterpret_cast<const KT*>(st + a.sl.key1)[i];
+                if (has_vals) v = reinterpret_cast<const VT*>(st + a.sl.val)[i];
+                if constexpr (NULLS) {
+                    const int wi = i >> 6, bb = i & 63;
+                    if (a.sl.knull0 >= 0) kn0 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull0)[wi] >> bb) & 1;
+                    if (a.sl.knull1 >= 0) kn1 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull1)[wi] >> bb) & 1;
+                    if (a.sl.vnull >= 0) vn = (reinterpret_cast<const uint64_t*>(st + a.sl.vnull)[wi] >> bb) & 1;
+                }
+            } else {
+                const int64_t r = base + i;
+                k0 = static_cast<const KT*>(a.key0)[r];
+                if constexpr (COMP) k1 = static_cast<const KT*>(a.key1)[r];
+                if (has_vals) v = static_cast<const VT*>(a.vals)[r];
+                if constexpr (NULLS) {
+                    kn0 = null_bit(a.knull0, r);
+                    kn1 = null_bit(a.knull1, r);
+                    vn = null_bit(a.vnull, r);
+                }
+            }
+            uint64_t kw = 0;
+            int kind = KK_NORMAL;
+            if constexpr (COMP) {
+                if (kn0 || kn1) {
+                    kind = KK_AUX;
+                    const uint32_t other = kn0 ? (kn1 ? 0u : static_cast<uint32_t>(k1)) : static_cast<uint32_t>(k0);
+                    kw = (static_cast<uint64_t>((kn0 ? 1u : 0u) | (kn1 ? 2u : 0u)) << 32) | other;
+                } else {
+                    kw = composite_word(static_cast<int32_t>(k0), static_cast<int32_t>(k1));
+                    kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                }
+            } else {
+                if (kn0) {
+                    kind = KK_NULL;
+                } else {
+                    kw = key_word(k0);
+                    kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
+                }
+            }
+            const bool agg_it = !has_vals || !vn;
+            bool inwin = true;
+            long long qv = 0;
+            if (agg_it && has_vals && a.has_sum) qv = sum_addend<VT>(v, fs, &inwin);
+            kw_out = kw;
+            v_out = v;
+            meta_out = static_cast<uint32_t>(kind) | (agg_it ? 4u : 0u);
+            if (!use_smem || kind == KK_AUX || !inwin) return true;
+            int slot_s;
+            if (kind == KK_NORMAL) {
+                const uint32_t h = bucket_home(kw, smem_shift);
+                bool found = false;
+                slot_s = s_find(tab.key, S, a.probe, kw, h, &found);
+                if (!spill_on) {
+                    ++my_tries;
+                    my_hits += found ? 1u : 0u;
+                }
+            } else {
+                slot_s = S + (kind == KK_ESCAPE ? 1 : 0);
+                if (*reinterpret_cast<volatile uint64_t*>(&tab.key[slot_s]) == kEmpty)
+                    atomicCAS(reinterpret_cast<unsigned long long*>(&tab.key[slot_s]), kEmpty, 0ull);
+            }
+            if (slot_s >= 0) {
+                if (agg_it) s_add<VT>(tab, a, slot_s, v, qv, has_vals);
+                return false;
+            }
+            if (spill_on && kind == KK_NORMAL && agg_it) {
+                const int p = a.spill_bits ? static_cast<int>((kw * 0x9e3779b97f4a7c15ull) >> (64 - a.spill_bits)) : 0;
+                const unsigned pos = atomicAdd(&sfill[p], 1u);
+                if (pos < cell_cap) {
+                    const int64_t idx = p * pstride + cell_off + pos;
+                    a.spill_keys[idx] = kw;
+                    if (has_vals) spill_v[idx] = v;
+                    return false;
+                }
+            }
+            return true;
+        };
+        // Queues row (kw, v, meta) of a lane whose `miss` is set; drains 32 rows when the queue is nearly full.
+        auto enqueue = [&](bool miss, uint64_t kw, VT v, uint32_t meta) {
+            const uint32_t mb = __ballot_sync(0xffffffffu, miss);
+            if (mb == 0u) return;
+            if (miss) {
+                const int pos = qn + __popc(mb & lt_mask);
+                qkw[pos] = kw;
+                uint64_t vb = 0;
+                memcpy(&vb, &v, sizeof(VT));
+                qval[pos] = vb;
+                qmeta[pos] = meta;
+            }
+            qn += __popc(mb);
+            if (qn > kQueueCap - 32) {  // keep room for the next batch
+                __syncwarp();
+                qn -= 32;
+                drain32(qn);
+                __syncwarp();
+            }
+        };
+        // The common case (one key column, no NULL masks, a staged tile) with few divergent regions per batch:
+        // every lane loads its row and probes the key's home slot; only lanes that did not find their key there
+        // run the full probe, only missing lanes take the spill / queue path.
+        auto fast_row = [&](int e0, const unsigned char* st, int count) {
+            const int e = e0 + lane;
+            const bool act = e < count;
+            const int i = list[act ? e : e0];
+            const uint64_t kw = key_word(reinterpret_cast<const KT*>(st + a.sl.key0)[i]);
+            const VT v = has_vals ? reinterpret_cast<const VT*>(st + a.sl.val)[i] : VT{};
+            bool inwin = true;
+            long long qv = 0;
+            if (a.has_sum) qv = sum_addend<VT>(v, fs, &inwin);
+            const bool normal = kw != kEmpty;
+            const uint32_t h0 = use_smem ? bucket_home(kw, smem_shift) : 0u;
+            const bool ok = act && normal && inwin && use_smem;
+            bool has_empty = false;
+            int slot = ok ? probe4(tab.ak, h0, kw, &has_empty) : -1;
+            bool hit = slot >= 0;
+            const bool need = ok && !hit && (has_empty || a.probe > 4);
+            if (__any_sync(0xffffffffu, need)) {
+                if (need) {
+                    bool found = false;
+                    slot = s_find32(tab.ak, S, a.probe, kw, h0, &found);
+                    hit = slot >= 0;
+                    if (!spill_on) {
+                        ++my_tries;
+                        my_hits += found ? 1u : 0u;
+                    }
+                }
+            }
+            if (hit) s_add<VT>(tab, a, slot, v, qv, has_vals);
+            bool miss = act && !hit;
+            if (__any_sync(0xffffffffu, miss)) {
+                if (miss && spill_on && normal && inwin) {
+                    const int p = a.spill_bits ? static_cast<int>((kw * 0x9e3779b97f4a7c15ull) >> (64 - a.spill_bits)) : 0;
+                    const unsigned pos = atoms_add(sfill_a + static_cast<uint32_t>(p) * 4u, 1u);
+                    if (pos < cell_cap) {
+                        const int64_t idx = p * pstride + cell_off + pos;
+                        a.spill_keys[idx] = kw;
+                        if (has_vals) spill_v[idx] = v;
+                        miss = false;
+                    }
+                }
+                enqueue(miss, kw, v, static_cast<uint32_t>(normal ? KK_NORMAL : KK_ESCAPE) | 4u);
+            }
+        };
+        int s = 0;
+        uint32_t ph = 0;
+        bool skip = false;
+        int64_t tile = blockIdx.x;
+        for (int64_t q = 0; q < my_tiles; ++q, tile += gridDim.x) {
             const bool staged = a.staged && tile < a.full_tiles;
-            const int s = static_cast<int>(q % a.NS);
-            if (staged && !mbar_wait(&full_bar[s], static_cast<uint32_t>((q / a.NS) & 1), a.counters)) break;
+            if (staged && !mbar_wait(&full_bar[s], ph, a.counters)) break;
             const unsigned char* st = sm + a.so_stage + static_cast<size_t>(s) * a.sl.bytes;
             const int64_t base = tile * T;
-            const bool skip = ((q & 15) == 0) && __any_sync(0xffffffffu, table_full(a.counters));
-            // Phase A: filter and compact.
+            if ((q & 31) == 0) skip = __any_sync(0xffffffffu, table_full(a.counters));
+            // Phase A: filter and compact.  Lane l evaluates the K = R/32 consecutive rows [l*K, (l+1)*K) of the
+            // warp's slice (vector loads from the stage); one ballot per row position ranks the passing rows into
+            // the warp's list.
             int count = 0;
-            for (int j = 0; j < R && !skip; j += 32) {
-                const int i = warp * R + j + lane;
-                const int64_t r = base + i;
-                bool keep = r < a.n;
-                if (keep) {
-                    if (a.mask) keep = (staged ? reinterpret_cast<const int8_t*>(st + a.sl.mask)[i] : a.mask[r]) != 0;
-                    if constexpr (HAS_PRED) {
-                        const PL pv = staged ? reinterpret_cast<const PL*>(st + a.sl.pred)[i]
-                                             : static_cast<const PL*>(a.pcol)[r];
-                        keep = keep && (((pv >= plo) && (pv <= phi)) != pinv);
-                        if constexpr (NULLS) {
-                            if (a.pnull) {
-                                const bool pn = staged ? ((reinterpret_cast<const uint64_t*>(st + a.sl.pnull)[i >> 6] >> (i & 63)) & 1)
-                                                       : null_bit(a.pnull, r);
-                                keep = keep && !pn;
+            if (!skip) {
+                const int i0 = warp * R + lane * K;
+                uint32_t bits = 0;
+                if (staged && HAS_PRED && !a.mask && !NULLS) {
+                    const PL* pp = reinterpret_cast<const PL*>(st + a.sl.pred) + i0;
+                    if constexpr (sizeof(PL) == 4) {
+                        if (K == 2) {
+                            const int2 w2 = *reinterpret_cast<const int2*>(pp);
+                            const PL p0 = from_bits<PL>(w2.x), p1 = from_bits<PL>(w2.y);
+                            bits = ((((p0 >= plo) && (p0 <= phi)) != pinv) ? 1u : 0u) |
+                                   ((((p1 >= plo) && (p1 <= phi)) != pinv) ? 2u : 0u);
+                        }
+                        for (int j = 0; K >= 4 && j < K; j += 4) {
+                            const int4 w4 = *reinterpret_cast<const int4*>(pp + j);
+                            const int32_t wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                const PL pv = from_bits<PL>(wv[u]);
+                                bits |= (((pv >= plo) && (pv <= phi)) != pinv ? 1u : 0u) << (j + u);
+                            }
+                        }
+                    } else {
+                        for (int j = 0; j < K; j += 2) {
+                            const int4 w4 = *reinterpret_cast<const int4*>(pp + j);
+                            const int64_t wv[2] = {(static_cast<int64_t>(static_cast<uint32_t>(w4.y)) << 32) | static_cast<uint32_t>(w4.x),
+                                                   (static_cast<int64_t>(static_cast<uint32_t>(w4.w)) << 32) | static_cast<uint32_t>(w4.z)};
+#pragma unroll
+                            for (int u = 0; u < 2; ++u) {
+                                const PL pv = from_bits<PL>(wv[u]);
+                                bits |= (((pv >= plo) && (pv <= phi)) != pinv ? 1u : 0u) << (j + u);
                             }
                         }
                     }
+                } else if (staged && !HAS_PRED && !a.mask) {
+                    bits = (K >= 32) ? 0xffffffffu : ((1u << K) - 1u);
+                } else {
+                    for (int j = 0; j < K; ++j) {
+                        const int i = i0 + j;
+                        const int64_t r = base + i;
+                        bool keep = r < a.n;
+                        if (keep) {
+                            if (a.mask) keep = (staged ? reinterpret_cast<const int8_t*>(st + a.sl.mask)[i] : a.mask[r]) != 0;
+                            if constexpr (HAS_PRED) {
+                                const PL pv = staged ? reinterpret_cast<const PL*>(st + a.sl.pred)[i]
+                                                     : static_cast<const PL*>(a.pcol)[r];
+                                keep = keep && (((pv >= plo) && (pv <= phi)) != pinv);
+                                if constexpr (NULLS) {
+                                    if (a.pnull) {
+                                        const bool pn = staged ? ((reinterpret_cast<const uint64_t*>(st + a.sl.pnull)[i >> 6] >> (i & 63)) & 1)
+                                                               : null_bit(a.pnull, r);
+                                        keep = keep && !pn;
+                                    }
+                                }
+                            }
+                        }
+                        bits |= (keep ? 1u : 0u) << j;
+                    }
                 }
-                const uint32_t b = __ballot_sync(0xffffffffu, keep);
-                if (keep) list[count + __popc(b & lt_mask)] = static_cast<uint16_t>(i);
-                count += __popc(b);
+                for (int j = 0; j < K; ++j) {
+                    const bool kj = (bits >> j) & 1u;
+                    const uint32_t bj = __ballot_sync(0xffffffffu, kj);
+                    if (kj) list[count + __popc(bj & lt_mask)] = static_cast<uint16_t>(i0 + j);
+                    count += __popc(bj);
+                }
             }
             __syncwarp();
-            // Phase B: insert the passing rows into the shared-memory table; rows that miss it are queued
-            // and inserted into the global table 32 at a time, so the L2 round trips of a warp overlap.
-            for (int e0 = 0; e0 < count; e0 += 32) {
-                const int e = e0 + lane;
-                const bool act = e < count;
-                uint64_t kw = 0;
-                int kind = KK_NORMAL;
-                bool agg_it = false;
-                VT v = VT{};
-                if (act) {
-                    const int i = list[e];
-                    const int64_t r = base + i;
-                    KT k0, k1 = KT{};
-                    bool kn0 = false, kn1 = false, vn = false;
-                    if (staged) {
-                        k0 = reinterpret_cast<const KT*>(st + a.sl.key0)[i];
-                        if constexpr (COMP) k1 = reinterpret_cast<const KT*>(st + a.sl.key1)[i];
-                        if (has_vals) v = reinterpret_cast<const VT*>(st + a.sl.val)[i];
-                        if constexpr (NULLS) {
-                            const int wi = i >> 6, bb = i & 63;
-                            if (a.sl.knull0 >= 0) kn0 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull0)[wi] >> bb) & 1;
-                            if (a.sl.knull1 >= 0) kn1 = (reinterpret_cast<const uint64_t*>(st + a.sl.knull1)[wi] >> bb) & 1;
-                            if (a.sl.vnull >= 0) vn = (reinterpret_cast<const uint64_t*>(st + a.sl.vnull)[wi] >> bb) & 1;
-                        }
-                    } else {
-                        k0 = static_cast<const KT*>(a.key0)[r];
-                        if constexpr (COMP) k1 = static_cast<const KT*>(a.key1)[r];
-                        if (has_vals) v = static_cast<const VT*>(a.vals)[r];
-                        if constexpr (NULLS) {
-                            kn0 = null_bit(a.knull0, r);
-                            kn1 = null_bit(a.knull1, r);
-                            vn = null_bit(a.vnull, r);
-                        }
-                    }
-                    if constexpr (COMP) {
-                        if (kn0 || kn1) {
-                            kind = KK_AUX;
-                            const uint32_t other =
-                                kn0 ? (kn1 ? 0u : static_cast<uint32_t>(k1)) : static_cast<uint32_t>(k0);
-                            kw = (static_cast<uint64_t>((kn0 ? 1u : 0u) | (kn1 ? 2u : 0u)) << 32) | other;
-                        } else {
-                            kw = composite_word(static_cast<int32_t>(k0), static_cast<int32_t>(k1));
-                            kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
-                        }
-                    } else {
-                        if (kn0) {
-                            kind = KK_NULL;
-                        } else {
-                            kw = key_word(k0);
-                            kind = (kw == kEmpty) ? KK_ESCAPE : KK_NORMAL;
-                        }
-                    }
-                    agg_it = !has_vals || !vn;
-                }
-                bool miss = act;
-                // Rows of the warp's hot keys accumulate in this lane's registers: no probe, no atomic.
-                if (act && kind == KK_NORMAL && (kw == hk0 || kw == hk1)) {
-                    miss = false;
-                    if (agg_it) {
-                        const int j = (kw == hk0) ? 0 : 1;
-                        const AccT x = has_vals ? to_acc<VT>(v) : AccT{};
-                        const long long e = has_vals ? enc_any<VT>(v) : 0;
-                        if (j == 0) {
-                            hc0 += 1;
-                            ha0 += x;
-                            hmn0 = min(hmn0, e);
-                            hmx0 = max(hmx0, e);
-                        } else {
-                            hc1 += 1;
-                            ha1 += x;
-                            hmn1 = min(hmn1, e);
-                            hmx1 = max(hmx1, e);
-                        }
-                    }
-                } else if (act && use_smem && kind != KK_AUX) {
-                    int slot_s;
-                    if (kind == KK_NORMAL) {
-                        bool found = false;
-                        slot_s = s_find(skey, S, a.probe, kw, smem_hash(kw, smem_shift), &found);
-                        ++my_tries;
-                        my_hits += found ? 1u : 0u;
-                    } else {
-                        slot_s = S + (kind == KK_ESCAPE ? 1 : 0);
-                        if (*reinterpret_cast<volatile uint64_t*>(&skey[slot_s]) == kEmpty)
-                            atomicCAS(reinterpret_cast<unsigned long long*>(&skey[slot_s]), kEmpty, 0ull);
-                    }
-                    if (slot_s >= 0) {
-                        miss = false;
-                        if (agg_it) s_acc_row<VT>(sm, a, slot_s, v, has_vals);
-                    }
-                }
-                const uint32_t mb = __ballot_sync(0xffffffffu, miss);
-                if (miss) {
-                    const int pos = qn + __popc(mb & lt_mask);
-                    qkw[pos] = kw;
-                    uint64_t vb = 0;
-                    memcpy(&vb, &v, sizeof(VT));
-                    qval[pos] = vb;
-                    qmeta[pos] = static_cast<uint32_t>(kind) | (agg_it ? 4u : 0u);
-                }
-                qn += __popc(mb);
-                if (qn >= 32) {
-                    __syncwarp();
-                    qn -= 32;
-                    issue(qn + lane);
-                    complete();
-                    __syncwarp();
+            // Phase B: two passing rows per lane per step (their loads and probes overlap); a row whose key misses
+            // the shared table goes to the spill area or, without one, to this warp's queue of global inserts.
+            if (FASTROW && staged) {
+                for (int e0 = 0; e0 < count; e0 += 32) fast_row(e0, st, count);
+            } else {
+                for (int e0 = 0; e0 < count; e0 += 64) {
+                    const int ea = e0 + lane, eb = e0 + 32 + lane;
+                    uint64_t kwa = 0, kwb = 0;
+                    VT va = VT{}, vb = VT{};
+                    uint32_t ma = 0, mbm = 0;
+                    const bool missa = ea < count && insert_row(ea, st, staged, base, kwa, va, ma);
+                    const bool missb = eb < count && insert_row(eb, st, staged, base, kwb, vb, mbm);
+                    enqueue(missa, kwa, va, ma);
+                    enqueue(missb, kwb, vb, mbm);
                 }
             }
             if (staged) {
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty_bar[s]);
             }
-            if (q == kDecideTile && use_smem) {
+            // Global inserts after the stage is released, so a slow L2 round trip does not hold the ring.
+            while (qn >= 32) {
+                __syncwarp();
+                qn -= 32;
+                drain32(qn);
+                __syncwarp();
+            }
+            if (q == kDecideTile && use_smem && !spill_on) {
                 const unsigned hits = __reduce_add_sync(0xffffffffu, my_hits);
                 const unsigned tries = __reduce_add_sync(0xffffffffu, my_tries);
                 if (tries >= 256 && hits * 8u < tries) use_smem = false;
-                else pick_hot_keys();
+            }
+            if (++s == a.NS) {
+                s = 0;
+                ph ^= 1u;
             }
             __syncwarp();
         }
-        flush_hot(hk0, hc0, ha0, hmn0, hmx0);
-        flush_hot(hk1, hc1, ha1, hmn1, hmx1);
         __syncwarp();
-        complete();
         if (lane < qn) {
-            issue(lane);
-            complete();
+            // the last partial batch: lanes >= qn idle
+            const uint64_t kw = qkw[lane];
+            const uint64_t vb = qval[lane];
+            const uint32_t meta = qmeta[lane];
+            const int kind = static_cast<int>(meta & 3u);
+            uint64_t* slot;
+            if (kind == KK_NORMAL || kind == KK_AUX) {
+                const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
+                slot = g_find(Rg, W, kw, mix64(kw), a.counters, &s_claims);
+            } else {
+                slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, &s_claims);
+            }
+            if (slot && (meta & 4u)) {
+                if (has_vals) {
+                    VT v;
+                    memcpy(&v, &vb, sizeof(VT));
+                    g_acc_row<VT>(slot, a, v);
+                } else {
+                    g_count_row(slot, a.L);
+                }
+            }
         }
         __syncwarp();
     }
 
-    // Merge this CTA's shared-memory table into the global table.
+    // Merge this CTA's shared-memory table into the global table; close the spill chunks.
     __syncthreads();
-    if (S) {
-        const bool v32 = sizeof(VT) == 4;
-        const bool vfloat = std::is_floating_point<VT>::value;
-        for (int i = threadIdx.x; i < S2; i += blockDim.x) {
-            const uint64_t key = skey[i];
-            if (key == kEmpty) continue;
-            uint64_t* slot = (i < S) ? g_find(a.main, W, key, mix64(key), a.counters, &s_claims)
-                                     : g_special(a.main, W, i - S, &s_claims);
-            if (!slot) continue;
-            const unsigned long long c = reinterpret_cast<unsigned int*>(sm + a.so_cnt)[i];
-            const uint64_t sumbits = a.has_sum ? reinterpret_cast<unsigned long long*>(sm + a.so_sum)[i] : 0ull;
-            long long mn = 0, mx = 0;
-            if (has_mm) {
-                if (v32) {
-                    const int* w = reinterpret_cast<const int*>(sm + a.so_mn) + 2 * i;
-                    mn = w[0];
-                    mx = w[1];
-                } else {
-                    mn = reinterpret_cast<long long*>(sm + a.so_mn)[i];
-                    mx = reinterpret_cast<long long*>(sm + a.so_mx)[i];
-                }
-            }
-            g_merge(slot, a.L, a.has_sum, a.has_min, a.has_max, v32, vfloat, c, sumbits, mn, mx);
+    fs = fix_scale(s_emax == INT_MIN ? 0 : s_emax);  // the producer warp's threads merge slots too
+    if (S) s_flush<VT>(tab, a, S, fs, &s_claims);
+    if (spill_on)
+        for (int i = threadIdx.x; i < (1 << a.spill_bits); i += blockDim.x)
+            a.spill_fill[static_cast<int64_t>(i) * a.spill_ctas + blockIdx.x] = min(sfill[i], static_cast<unsigned>(a.spill_cell));
+    __syncthreads();
+    if (threadIdx.x == 0) publish_claims(a.counters, a.capacity, s_claims);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Second pass over the spill: CTA (p, j) aggregates cells j, j + slices, ... of partition p in a shared-memory
+// table (each warp walks whole cells, 64 rows per step with both loads issued first), sends the rows its table
+// cannot hold to the global table directly, and merges the table into the global table.
+// ---------------------------------------------------------------------------------------------
+// One spilled row per lane (act: the lane has a row): home-slot probe, full probe only for lanes that need it,
+// slot update, and the global table for rows the shared table cannot take.
+template <typename VT>
+__device__ __forceinline__ void spill_rows(const STable& tab, const AggArgs& a, const FixScale& fs, int S, int shift,
+                                           bool act, uint64_t kw, VT v, bool has_vals, unsigned long long* claims) {
+    bool inwin = true;
+    long long qv = 0;
+    if (has_vals && a.has_sum) qv = sum_addend<VT>(v, fs, &inwin);
+    const uint32_t h0 = bucket_home(kw, shift);
+    const bool ok = act && inwin;
+    bool has_empty = false;
+    int slot = ok ? probe4(tab.ak, h0, kw, &has_empty) : -1;
+    bool hit = slot >= 0;
+    const bool need = ok && !hit && (has_empty || a.probe > 4);
+    if (__any_sync(0xffffffffu, need)) {
+        if (need) {
+            bool found = false;
+            slot = s_find32(tab.ak, S, a.probe, kw, h0, &found);
+            hit = slot >= 0;
         }
     }
+    if (hit) s_add<VT>(tab, a, slot, v, qv, has_vals);
+    const bool miss = act && !hit;
+    if (__any_sync(0xffffffffu, miss)) {
+        if (miss) {
+            uint64_t* g = g_find(a.main, a.L.W, kw, mix64(kw), a.counters, claims);
+            if (g) {
+                if (has_vals) g_acc_row<VT>(g, a, v);
+                else g_count_row(g, a.L);
+            }
+        }
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kSpillThreads) gb_spill_kernel(const AggArgs a) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    __shared__ unsigned long long s_claims;
+    __shared__ int s_emax;
+    constexpr bool VFLOAT = std::is_floating_point<VT>::value;
+    const int S = a.S;
+    const STable tab = stable(sm, a);
+    const int parts = 1 << a.spill_bits;
+    const int p = static_cast<int>(blockIdx.x % parts);
+    const int j = static_cast<int>(blockIdx.x / parts);
+    const int slices = static_cast<int>(gridDim.x / parts);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const bool has_vals = a.spill_vals != nullptr;
+    s_init<VT>(tab, a, S + 2);
+    if (threadIdx.x == 0) {
+        s_claims = 0;
+        s_emax = INT_MIN;
+    }
+    __syncthreads();
+    const int64_t cell0 = static_cast<int64_t>(p) * a.spill_ctas;
+    const int cstep = slices * nwarps;
+    if (VFLOAT && a.has_sum && has_vals) {  // scale from the first rows of each warp's first cell
+        int e = INT_MIN;
+        const int c = j + slices * warp;
+        if (c < a.spill_ctas) {
+            const int f = static_cast<int>(a.spill_fill[cell0 + c]);
+            if (lane < f) e = value_exp<VT>(static_cast<const VT*>(a.spill_vals)[(cell0 + c) * a.spill_cell + lane]);
+        }
+        e = __reduce_max_sync(0xffffffffu, e);
+        if (lane == 0 && e != INT_MIN) atomicMax(&s_emax, e);
+    }
+    __syncthreads();
+    const FixScale fs = fix_scale(s_emax == INT_MIN ? 0 : s_emax);
+    const int shift = 32 - (31 - __clz(S));
+    for (int c = j + slices * warp; c < a.spill_ctas; c += cstep) {
+        const int f = static_cast<int>(a.spill_fill[cell0 + c]);
+        const int64_t base = (cell0 + c) * a.spill_cell;
+        const uint64_t* keys = a.spill_keys + base;
+        const VT* vals = has_vals ? static_cast<const VT*>(a.spill_vals) + base : nullptr;
+        for (int r0 = 0; r0 < f; r0 += 64) {
+            const int ra = r0 + lane, rb = r0 + 32 + lane;
+            const bool aa = ra < f, ab = rb < f;
+            const uint64_t k0 = aa ? keys[ra] : 0ull;
+            const uint64_t k1 = ab ? keys[rb] : 0ull;
+            const VT v0 = (has_vals && aa) ? vals[ra] : VT{};
+            const VT v1 = (has_vals && ab) ? vals[rb] : VT{};
+            spill_rows<VT>(tab, a, fs, S, shift, aa, k0, v0, has_vals, &s_claims);
+            if (r0 + 32 < f) spill_rows<VT>(tab, a, fs, S, shift, ab, k1, v1, has_vals, &s_claims);
+        }
+    }
+    __syncthreads();
+    s_flush<VT>(tab, a, S, fs, &s_claims);
     __syncthreads();
     if (threadIdx.x == 0) publish_claims(a.counters, a.capacity, s_claims);
 }
@@ -812,10 +1265,29 @@ int32_t launch_agg_t(const AggArgs& a, size_t smem, cudaStream_t st) {
     int64_t grid = static_cast<int64_t>(di.sm_count) * per_sm;
     if (grid > a.tiles) grid = a.tiles;
     if (grid < 1) return QDB_OK;
+    if (a.spill_keys) {  // the spill cells are laid out for exactly spill_ctas CTAs
+        if (a.spill_ctas > grid) return fail(QDB_ERROR, "gb_agg_kernel: spill plan needs more CTAs than fit");
+        grid = a.spill_ctas;
+    }
     kern<<<static_cast<unsigned>(grid), kAggThreads, smem, st>>>(a);
     note_launch();
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "gb_agg_kernel launch");
+    return QDB_OK;
+}
+
+// Launches the spill pass (grid = partitions x slices).
+template <typename VT>
+int32_t launch_spill_t(const AggArgs& a, size_t smem, int64_t grid, cudaStream_t st) {
+    auto kern = gb_spill_kernel<VT>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(gb_spill_kernel)");
+    }
+    kern<<<static_cast<unsigned>(grid), kSpillThreads, smem, st>>>(a);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "gb_spill_kernel launch");
     return QDB_OK;
 }
 
