@@ -37,12 +37,11 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait on phase `parity`; gives up after kMaxWaitIters tries and records QDB_ERR_TIMEOUT in *err.
+// Bounded wait on phase `parity`; gives up after kMaxWaitIters tries (each suspends up to 10 us) and records
+// QDB_ERR_TIMEOUT in *err.
 __device__ __forceinline__ bool b_wait(uint64_t* bar, uint32_t parity, int32_t* err) {
-    for (uint32_t it = 0; it < kMaxWaitIters; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (it >= 16) __nanosleep(64);
-    }
+    for (uint32_t it = 0; it < kMaxWaitIters; ++it)
+        if (mbar_try_wait_for(bar, parity, 10000u)) return true;
     atomicExch(err, static_cast<int>(QDB_ERR_TIMEOUT));
     return false;
 }

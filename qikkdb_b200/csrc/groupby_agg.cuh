@@ -36,7 +36,7 @@ constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsume
 constexpr int kQueueCap = 64;                              // per-warp queue of rows for the global table
 constexpr int kSpillThreads = 512;                         // threads of a spill-pass CTA
 constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
-constexpr uint32_t kMaxWaitIters = 1u << 24;               // bounded mbarrier waits (seconds, then give up)
+constexpr uint32_t kMaxWaitIters = 1u << 18;               // bounded mbarrier waits (seconds, then give up)
 
 // `col OP constant` as an interval of the column type: keep = (lo <= x && x <= hi) != invert.
 struct PredInterval {
@@ -181,12 +181,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Waits for phase `parity` of `bar`; gives up after kMaxWaitIters tries and records QDB_ERR_TIMEOUT.
+// try_wait with a suspend-time hint: the warp sleeps in hardware until the phase completes or about `ns` pass,
+// so a waiting warp issues no instructions while it waits.
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `parity` of `bar`; gives up after kMaxWaitIters tries (each suspends up to 10 us, so about
+// 2.6 s in all) and records QDB_ERR_TIMEOUT.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long* counters) {
-    for (uint32_t it = 0; it < kMaxWaitIters; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if (it >= 16) __nanosleep(128);
-    }
+    for (uint32_t it = 0; it < kMaxWaitIters; ++it)
+        if (mbar_try_wait_for(bar, parity, 10000u)) return true;
     atomicExch(reinterpret_cast<int*>(&counters[1]), static_cast<int>(QDB_ERR_TIMEOUT));
     return false;
 }
