@@ -644,42 +644,65 @@ __device__ __forceinline__ void s_init(const STable& t, const AggArgs& a, int S2
 }
 
 // Merges every occupied slot of a shared table into the global table (whole CTA).
+// Merges one occupied shared slot i into global slot g.
 template <typename VT>
-__device__ __forceinline__ void s_flush(const STable& t, const AggArgs& a, int S, const FixScale& fs,
-                                        unsigned long long* claims) {
+__device__ __forceinline__ void s_merge_slot(const STable& t, const AggArgs& a, int i, uint64_t* g, const FixScale& fs) {
     const bool has_mm = a.has_min || a.has_max;
     const bool v32 = sizeof(VT) == 4;
     const bool vfloat = std::is_floating_point<VT>::value;
+    const unsigned long long c = t.cnt[i];
+    uint64_t sumbits = 0;
+    if (a.has_sum) {
+        if (vfloat) {
+            const double d = limbs96_to_double(t.l0[i], t.l1[i], t.l2[i]) * fs.inv;
+            memcpy(&sumbits, &d, 8);
+        } else {
+            sumbits = (static_cast<uint64_t>(t.l1[i]) << 32) | t.l0[i];
+        }
+    }
+    long long mn = 0, mx = 0;
+    if (has_mm) {
+        if (v32) {
+            const int* w = reinterpret_cast<const int*>(t.mm) + 2 * i;
+            mn = w[0];
+            mx = w[1];
+        } else {
+            const long long* w = reinterpret_cast<const long long*>(t.mm) + 2 * i;
+            mn = w[0];
+            mx = w[1];
+        }
+    }
+    g_merge(g, a.L, a.has_sum, a.has_min, a.has_max, v32, vfloat, c, sumbits, mn, mx);
+}
+
+// Merges every occupied slot of a shared table into the global table (whole CTA).  Each thread takes four
+// slots at a time and issues the four home-slot loads of the global table before resolving any of them, so
+// the L2 round trips overlap.
+template <typename VT>
+__device__ __forceinline__ void s_flush(const STable& t, const AggArgs& a, int S, const FixScale& fs,
+                                        unsigned long long* claims) {
     const int W = a.L.W;
-    for (int i = threadIdx.x; i < S + 2; i += blockDim.x) {
-        const uint64_t key = t.key[i];
-        if (key == kEmpty) continue;
-        uint64_t* slot = (i < S) ? g_find(a.main, W, key, mix64(key), a.counters, claims)
-                                 : g_special(a.main, W, i - S, claims);
-        if (!slot) continue;
-        const unsigned long long c = t.cnt[i];
-        uint64_t sumbits = 0;
-        if (a.has_sum) {
-            if (vfloat) {
-                const double d = limbs96_to_double(t.l0[i], t.l1[i], t.l2[i]) * fs.inv;
-                memcpy(&sumbits, &d, 8);
-            } else {
-                sumbits = (static_cast<uint64_t>(t.l1[i]) << 32) | t.l0[i];
-            }
+    constexpr int U = 4;
+    for (int i0 = threadIdx.x; i0 < S; i0 += U * blockDim.x) {
+        uint64_t key[U], pos[U], cur[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * blockDim.x;
+            key[u] = (i < S) ? t.key[i] : kEmpty;
+            pos[u] = mix64(key[u]) & a.main.mask;
         }
-        long long mn = 0, mx = 0;
-        if (has_mm) {
-            if (v32) {
-                const int* w = reinterpret_cast<const int*>(t.mm) + 2 * i;
-                mn = w[0];
-                mx = w[1];
-            } else {
-                const long long* w = reinterpret_cast<const long long*>(t.mm) + 2 * i;
-                mn = w[0];
-                mx = w[1];
-            }
+#pragma unroll
+        for (int u = 0; u < U; ++u) cur[u] = (key[u] != kEmpty) ? ld_volatile_u64(a.main.slots + pos[u] * W) : 0ull;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (key[u] == kEmpty) continue;
+            uint64_t* g = g_find_from(a.main, W, key[u], pos[u], cur[u], a.counters, claims);
+            if (g) s_merge_slot<VT>(t, a, i0 + u * blockDim.x, g, fs);
         }
-        g_merge(slot, a.L, a.has_sum, a.has_min, a.has_max, v32, vfloat, c, sumbits, mn, mx);
+    }
+    if (threadIdx.x < 2 && t.key[S + threadIdx.x] != kEmpty) {  // the NULL-key and escaped-key slots
+        uint64_t* g = g_special(a.main, W, static_cast<int>(threadIdx.x), claims);
+        if (g) s_merge_slot<VT>(t, a, S + threadIdx.x, g, fs);
     }
 }
 
@@ -1244,15 +1267,18 @@ __global__ void __launch_bounds__(kSpillThreads) gb_spill_kernel(const AggArgs a
         const int64_t base = (cell0 + c) * a.spill_cell;
         const uint64_t* keys = a.spill_keys + base;
         const VT* vals = has_vals ? static_cast<const VT*>(a.spill_vals) + base : nullptr;
-        for (int r0 = 0; r0 < f; r0 += 64) {
-            const int ra = r0 + lane, rb = r0 + 32 + lane;
-            const bool aa = ra < f, ab = rb < f;
-            const uint64_t k0 = aa ? keys[ra] : 0ull;
-            const uint64_t k1 = ab ? keys[rb] : 0ull;
-            const VT v0 = (has_vals && aa) ? vals[ra] : VT{};
-            const VT v1 = (has_vals && ab) ? vals[rb] : VT{};
-            spill_rows<VT>(tab, a, fs, S, shift, aa, k0, v0, has_vals, &s_claims);
-            if (r0 + 32 < f) spill_rows<VT>(tab, a, fs, S, shift, ab, k1, v1, has_vals, &s_claims);
+        for (int r0 = 0; r0 < f; r0 += 128) {  // four rows per lane: all their loads are issued first
+            uint64_t k[4];
+            VT v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = r0 + 32 * u + lane;
+                k[u] = r < f ? keys[r] : 0ull;
+                v[u] = (has_vals && r < f) ? vals[r] : VT{};
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (r0 + 32 * u < f) spill_rows<VT>(tab, a, fs, S, shift, r0 + 32 * u + lane < f, k[u], v[u], has_vals, &s_claims);
         }
     }
     __syncthreads();
