@@ -297,7 +297,7 @@ def run_ours(args):
     achieved = n * BYTES_PER_ROW / t_agg / 1e9
     traffic = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "gb_agg_kernel (fused filter + hash aggregate)",
+                "traffic": traffic, "kernel": "gb_agg_kernel + gb_spill_kernel (fused filter + shared-table aggregate, spill merge)",
                 "kernel_ms": t_agg * 1e3, "algorithmic_bytes_per_launch": n * BYTES_PER_ROW,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
     cpu = cpu_baseline(cols, args.cpu_sample_rows) if (rank == 0 and world == 1) else None
