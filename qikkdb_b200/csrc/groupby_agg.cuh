@@ -1232,6 +1232,7 @@ __global__ void __launch_bounds__(kSpillThreads) gb_spill_kernel(const AggArgs a
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ unsigned long long s_claims;
     __shared__ int s_emax;
+    __shared__ int s_next_cell;
     constexpr bool VFLOAT = std::is_floating_point<VT>::value;
     const int S = a.S;
     const STable tab = stable(sm, a);
@@ -1239,16 +1240,17 @@ __global__ void __launch_bounds__(kSpillThreads) gb_spill_kernel(const AggArgs a
     const int p = static_cast<int>(blockIdx.x % parts);
     const int j = static_cast<int>(blockIdx.x / parts);
     const int slices = static_cast<int>(gridDim.x / parts);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool has_vals = a.spill_vals != nullptr;
     s_init<VT>(tab, a, S + 2);
     if (threadIdx.x == 0) {
         s_claims = 0;
         s_emax = INT_MIN;
+        s_next_cell = 0;
     }
     __syncthreads();
     const int64_t cell0 = static_cast<int64_t>(p) * a.spill_ctas;
-    const int cstep = slices * nwarps;
+    const int ncells = (a.spill_ctas - j + slices - 1) / slices;  // cells j, j + slices, ... of this partition
     if (VFLOAT && a.has_sum && has_vals) {  // scale from the first rows of each warp's first cell
         int e = INT_MIN;
         const int c = j + slices * warp;
@@ -1262,7 +1264,12 @@ __global__ void __launch_bounds__(kSpillThreads) gb_spill_kernel(const AggArgs a
     __syncthreads();
     const FixScale fs = fix_scale(s_emax == INT_MIN ? 0 : s_emax);
     const int shift = 32 - (31 - __clz(S));
-    for (int c = j + slices * warp; c < a.spill_ctas; c += cstep) {
+    for (;;) {  // warps take the next cell from a shared counter, so uneven cells do not leave warps idle
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&s_next_cell, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= ncells) break;
+        const int c = j + slices * t;
         const int f = static_cast<int>(a.spill_fill[cell0 + c]);
         const int64_t base = (cell0 + c) * a.spill_cell;
         const uint64_t* keys = a.spill_keys + base;
