@@ -850,11 +850,34 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
         int qn = 0;
         // Global inserts of queued rows, 32 at a time with every lane active, so the warp's 32 probe loads
         // are in flight together.
-        auto drain32 = [&](int first) {
+        // Spill cell addressing of this CTA: row pos of partition p is at p * pstride + cell_off + pos.
+        const int64_t pstride = spill_on ? static_cast<int64_t>(a.spill_ctas) * a.spill_cell : 0;
+        const int64_t cell_off = spill_on ? static_cast<int64_t>(blockIdx.x) * a.spill_cell : 0;
+        const unsigned cell_cap = spill_on ? static_cast<unsigned>(a.spill_cell) : 0u;
+        VT* const spill_v = static_cast<VT*>(a.spill_vals);
+        const uint32_t sfill_a = smem_u32(sfill);
+        // Rows of the warp's queue, lanes < nvalid taking entries first + lane: a spillable row (meta bit 8) is
+        // appended to its partition's cell, every other row (and a row whose cell is full) is inserted into the
+        // global table.  A whole warp handles the queue at once, so the spill stores and the global probe loads of
+        // up to 32 rows are in flight together.
+        auto drain = [&](int first, int nvalid) {
+            if (lane >= nvalid) return;
             const int e = first + lane;
             const uint64_t kw = qkw[e];
             const uint64_t vb = qval[e];
             const uint32_t meta = qmeta[e];
+            VT v;
+            memcpy(&v, &vb, sizeof(VT));
+            if (meta & 8u) {
+                const int p = a.spill_bits ? static_cast<int>((kw * 0x9e3779b97f4a7c15ull) >> (64 - a.spill_bits)) : 0;
+                const unsigned pos = atoms_add(sfill_a + static_cast<uint32_t>(p) * 4u, 1u);
+                if (pos < cell_cap) {
+                    const int64_t idx = p * pstride + cell_off + pos;
+                    a.spill_keys[idx] = kw;
+                    if (has_vals) spill_v[idx] = v;
+                    return;
+                }
+            }
             const int kind = static_cast<int>(meta & 3u);
             uint64_t* slot;
             if (kind == KK_NORMAL || kind == KK_AUX) {
@@ -864,21 +887,11 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, &s_claims);
             }
             if (slot && (meta & 4u)) {
-                if (has_vals) {
-                    VT v;
-                    memcpy(&v, &vb, sizeof(VT));
-                    g_acc_row<VT>(slot, a, v);
-                } else {
-                    g_count_row(slot, a.L);
-                }
+                if (has_vals) g_acc_row<VT>(slot, a, v);
+                else g_count_row(slot, a.L);
             }
         };
-        // Spill cell addressing of this CTA: row pos of partition p is at p * pstride + cell_off + pos.
-        const int64_t pstride = spill_on ? static_cast<int64_t>(a.spill_ctas) * a.spill_cell : 0;
-        const int64_t cell_off = spill_on ? static_cast<int64_t>(blockIdx.x) * a.spill_cell : 0;
-        const unsigned cell_cap = spill_on ? static_cast<unsigned>(a.spill_cell) : 0u;
-        VT* const spill_v = static_cast<VT*>(a.spill_vals);
-        const uint32_t sfill_a = smem_u32(sfill);
+        auto drain32 = [&](int first) { drain(first, 32); };
         const int K = R >> 5;  // rows per lane in phase A
         // One passing row (list entry e): probe the shared table, update the slot, or spill; returns true when the
         // row must go to the warp's queue of global inserts.
@@ -954,16 +967,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 if (agg_it) s_add<VT>(tab, a, slot_s, v, qv, has_vals);
                 return false;
             }
-            if (spill_on && kind == KK_NORMAL && agg_it) {
-                const int p = a.spill_bits ? static_cast<int>((kw * 0x9e3779b97f4a7c15ull) >> (64 - a.spill_bits)) : 0;
-                const unsigned pos = atomicAdd(&sfill[p], 1u);
-                if (pos < cell_cap) {
-                    const int64_t idx = p * pstride + cell_off + pos;
-                    a.spill_keys[idx] = kw;
-                    if (has_vals) spill_v[idx] = v;
-                    return false;
-                }
-            }
+            if (spill_on && kind == KK_NORMAL && agg_it) meta_out |= 8u;  // the queue drain spills it
             return true;
         };
         // Queues row (kw, v, meta) of a lane whose `miss` is set; drains 32 rows when the queue is nearly full.
@@ -1017,20 +1021,9 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 }
             }
             if (hit) s_add<VT>(tab, a, slot, v, qv, has_vals);
-            bool miss = act && !hit;
-            if (__any_sync(0xffffffffu, miss)) {
-                if (miss && spill_on && normal && inwin) {
-                    const int p = a.spill_bits ? static_cast<int>((kw * 0x9e3779b97f4a7c15ull) >> (64 - a.spill_bits)) : 0;
-                    const unsigned pos = atoms_add(sfill_a + static_cast<uint32_t>(p) * 4u, 1u);
-                    if (pos < cell_cap) {
-                        const int64_t idx = p * pstride + cell_off + pos;
-                        a.spill_keys[idx] = kw;
-                        if (has_vals) spill_v[idx] = v;
-                        miss = false;
-                    }
-                }
-                enqueue(miss, kw, v, static_cast<uint32_t>(normal ? KK_NORMAL : KK_ESCAPE) | 4u);
-            }
+            const bool miss = act && !hit;
+            const uint32_t spillable = (spill_on && normal && inwin) ? 8u : 0u;
+            enqueue(miss, kw, v, static_cast<uint32_t>(normal ? KK_NORMAL : KK_ESCAPE) | 4u | spillable);
         };
         int s = 0;
         uint32_t ph = 0;
@@ -1151,33 +1144,11 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             __syncwarp();
         }
         __syncwarp();
-        if (lane < qn) {
-            // the last partial batch: lanes >= qn idle
-            const uint64_t kw = qkw[lane];
-            const uint64_t vb = qval[lane];
-            const uint32_t meta = qmeta[lane];
-            const int kind = static_cast<int>(meta & 3u);
-            uint64_t* slot;
-            if (kind == KK_NORMAL || kind == KK_AUX) {
-                const Region& Rg = (kind == KK_AUX) ? a.aux : a.main;
-                slot = g_find(Rg, W, kw, mix64(kw), a.counters, &s_claims);
-            } else {
-                slot = g_special(a.main, W, kind == KK_ESCAPE ? 1 : 0, &s_claims);
-            }
-            if (slot && (meta & 4u)) {
-                if (has_vals) {
-                    VT v;
-                    memcpy(&v, &vb, sizeof(VT));
-                    g_acc_row<VT>(slot, a, v);
-                } else {
-                    g_count_row(slot, a.L);
-                }
-            }
-        }
+        drain(0, qn);  // the last partial batch: lanes >= qn idle
         __syncwarp();
     }
 
-    // Merge this CTA's shared-memory table into the global table; close the spill chunks.
+    // Merge this CTA's shared-memory table into the global table; publish the spill cell fills.
     __syncthreads();
     fs = fix_scale(s_emax == INT_MIN ? 0 : s_emax);  // the producer warp's threads merge slots too
     if (S) s_flush<VT>(tab, a, S, fs, &s_claims);
