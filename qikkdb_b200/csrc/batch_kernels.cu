@@ -89,19 +89,33 @@ __device__ __forceinline__ void b_s_acc(const BSmem& t, int s, VT v, bool has_va
     atomicAdd(t.cnt + s, 1u);
     if (!has_vals) return;
     if (has_sum) {
-        if constexpr (std::is_floating_point<VT>::value)
+        if constexpr (std::is_floating_point<VT>::value) {
             atomicAdd(reinterpret_cast<double*>(t.sum) + s, static_cast<double>(v));
-        else
-            atomicAdd(t.sum + s, static_cast<unsigned long long>(static_cast<long long>(v)));
+        } else {
+            // The 64-bit two's-complement add as two 32-bit shared atomics on the halves of the word (the carry out
+            // of the low half is read from the value its atomic returns): the same word as a 64-bit atomicAdd,
+            // without the 64-bit CAS loop that serialises when many lanes hit one slot.
+            const unsigned long long u = static_cast<unsigned long long>(static_cast<long long>(v));
+            unsigned* w = reinterpret_cast<unsigned*>(t.sum + s);
+            const unsigned x0 = static_cast<unsigned>(u), x1 = static_cast<unsigned>(u >> 32);
+            const unsigned old = atomicAdd(w, x0);
+            const unsigned hi = x1 + ((old + x0 < old) ? 1u : 0u);
+            if (hi) atomicAdd(w + 1, hi);
+        }
     }
+    // min/max: an atomic only when the value improves on the slot's current bound
     if constexpr (sizeof(VT) == 4) {
         const int32_t e = enc32(v);
-        if (has_min) atomicMin(reinterpret_cast<int*>(t.mn) + 2 * s, e);
-        if (has_max) atomicMax(reinterpret_cast<int*>(t.mx) + 2 * s + 1, e);
+        int* mn = reinterpret_cast<int*>(t.mn) + 2 * s;
+        int* mx = reinterpret_cast<int*>(t.mx) + 2 * s + 1;
+        if (has_min && e < *reinterpret_cast<volatile int*>(mn)) atomicMin(mn, e);
+        if (has_max && e > *reinterpret_cast<volatile int*>(mx)) atomicMax(mx, e);
     } else {
         const long long e = enc64(v);
-        if (has_min) atomicMin(reinterpret_cast<long long*>(t.mn) + s, e);
-        if (has_max) atomicMax(reinterpret_cast<long long*>(t.mx) + s, e);
+        long long* mn = reinterpret_cast<long long*>(t.mn) + s;
+        long long* mx = reinterpret_cast<long long*>(t.mx) + s;
+        if (has_min && e < *reinterpret_cast<volatile long long*>(mn)) atomicMin(mn, e);
+        if (has_max && e > *reinterpret_cast<volatile long long*>(mx)) atomicMax(mx, e);
     }
 }
 

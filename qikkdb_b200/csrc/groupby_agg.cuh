@@ -1034,7 +1034,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             if (staged && !mbar_wait(&full_bar[s], ph, a.counters)) break;
             const unsigned char* st = sm + a.so_stage + static_cast<size_t>(s) * a.sl.bytes;
             const int64_t base = tile * T;
-            if ((q & 31) == 0) skip = __any_sync(0xffffffffu, table_full(a.counters));
+            if ((q & 127) == 0) skip = __any_sync(0xffffffffu, table_full(a.counters));  // an L2 round trip: rarely
             // Phase A: filter and compact.  Lane l evaluates the K = R/32 consecutive rows [l*K, (l+1)*K) of the
             // warp's slice (vector loads from the stage); one ballot per row position ranks the passing rows into
             // the warp's list.
