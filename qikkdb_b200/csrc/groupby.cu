@@ -476,7 +476,8 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
             }
         }
     }
-    const size_t spill_words_bytes = spill_bits >= 0 ? ((size_t(4) << spill_bits) + 127) & ~size_t(127) : 0;
+    // spill cell fill counters, then a 32768-bit filter of keys seen once (admission to the shared table)
+    const size_t spill_words_bytes = spill_bits >= 0 ? ((size_t(4) << spill_bits) + kSeenWords * 4 + 127) & ~size_t(127) : 0;
     const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024 - stage_area - bar_bytes - list_bytes -
                           queue_bytes - spill_words_bytes;
 

@@ -35,6 +35,7 @@ constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer war
 constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsumerWarps * R rows, R a multiple of 64
 constexpr int kQueueCap = 64;                              // per-warp queue of rows for the global table
 constexpr int kSpillThreads = 512;                         // threads of a spill-pass CTA
+constexpr int kSeenWords = 1024;                           // 32768-bit filter of keys seen once (spilling tables)
 constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
 constexpr uint32_t kMaxWaitIters = 1u << 18;               // bounded mbarrier waits (seconds, then give up)
 
@@ -714,6 +715,8 @@ __device__ __forceinline__ void s_flush(const STable& t, const AggArgs& a, int S
 // Every CTA owns one cell of every partition, so an append is one 32-bit shared-memory atomic on the cell's
 // fill counter and two plain stores; a row that finds its cell full takes the global path instead.
 // ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool spill_keys_on(const AggArgs& a) { return a.spill_keys != nullptr; }
+
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type
 // (int32_t when the table has no value column); PT: predicate column type or NoPred; NULLS: some null
@@ -734,13 +737,14 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
     uint64_t* full_bar = reinterpret_cast<uint64_t*>(sm + a.so_bar);
     uint64_t* empty_bar = full_bar + a.NS;
     unsigned* sfill = reinterpret_cast<unsigned*>(sm + a.so_spill);
+    unsigned* seen = sfill + (spill_keys_on(a) ? (1 << a.spill_bits) : 0);
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const bool spill_on = a.spill_keys != nullptr;
 
     if (S) s_init<VT>(tab, a, S + 2);
     if (spill_on)
-        for (int i = threadIdx.x; i < (1 << a.spill_bits); i += blockDim.x) sfill[i] = 0u;
+        for (int i = threadIdx.x; i < (1 << a.spill_bits) + kSeenWords; i += blockDim.x) sfill[i] = 0u;
     if (threadIdx.x == 0) {
         s_claims = 0;
         s_emax = INT_MIN;
@@ -1010,7 +1014,15 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
             bool hit = slot >= 0;
             const bool need = ok && !hit && (has_empty || a.probe > 4);
             if (__any_sync(0xffffffffu, need)) {
-                if (need) {
+                // While the table fills, a spilling table admits a key on its second occurrence only (a bit
+                // filter of keys seen once), so the slots go to keys that recur rather than to the first comers.
+                bool admit = need;
+                if (need && spill_on) {
+                    const uint32_t hb = static_cast<uint32_t>((kw * 0xd6e8feb86659fd93ull) >> 49);
+                    const unsigned bit = 1u << (hb & 31u);
+                    admit = (atomicOr(&seen[hb >> 5], bit) & bit) != 0u;
+                }
+                if (admit) {
                     bool found = false;
                     slot = s_find32(tab.ak, S, a.probe, kw, h0, &found);
                     hit = slot >= 0;
