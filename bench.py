@@ -49,7 +49,7 @@ WORKLOAD = "filtered-groupby-256M: f32 pred p<0.5, int64 Zipf(1.1) keys over 1M,
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
@@ -80,9 +80,11 @@ def gen_columns(n: int, shard: int, pinned: bool):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms; `summary()` keeps the samples taken while the
+    timed region ran (from `__enter__` to `__exit__`).  `__enter__` waits for the sampler's first line before it
+    returns, so a short timed region still falls between samples that exist."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -90,6 +92,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.file = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -97,12 +100,18 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
+            deadline = time.time() + 5.0
+            while time.time() < deadline and os.path.getsize(self.file.name) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *exc):
+        self.t1 = time.time()
         if self.proc is not None:
+            time.sleep(0.12)  # one more sample after the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -110,20 +119,33 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
         if self.file is None:
             return None
         try:
-            rows = [r.split(",") for r in open(self.file.name).read().strip().splitlines() if r.strip()]
+            rows = [[c.strip() for c in r.split(",")] for r in open(self.file.name).read().strip().splitlines()
+                    if r.strip()]
             os.unlink(self.file.name)
         except Exception:
             return None
+        rows = [r for r in rows if len(r) > 9]
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if len(r) > 8]
-        mx = max(float(r[2]) for r in rows if len(r) > 8)
+
+        def stamp(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except Exception:
+                return None
+
+        inside = [r for r in rows if stamp(r) is not None and self.t0 - 0.05 <= stamp(r) <= self.t1 + 0.1]
+        use = inside or rows
+        sm = [float(r[2]) for r in use]
+        mx = max(float(r[3]) for r in use)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4) if r[5 + i].strip() == "Active"})
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for r in use for i in range(4) if r[6 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": reasons, "samples": len(use),
+                "window": "timed region" if inside else "whole sampler run (no sample inside the timed region)"}
 
 
 def measured_peak():

@@ -501,11 +501,13 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
         }
     }
     if (spill_bits >= 0) {
-        // Spill area: one cell per (partition, CTA).  A cell holds 5/4 of its share of this call's rows (at most
-        // 2^27) plus 64, so hashed misses overflow a cell only when nearly every row misses the shared table.
+        // Spill area: one cell per (partition, CTA).  A cell holds 5/4 of its share of half this call's rows (at
+        // most 2^28 rows in all) plus 64: warps whose shared-table hit rate is below 1/2 stop spilling, so hashed
+        // misses overflow a cell only in the first tiles of such warps (and rows of a full cell go to the global
+        // table).
         const int64_t parts = int64_t(1) << spill_bits;
         const int64_t ctas = std::min<int64_t>(di.sm_count, a.tiles);
-        const int64_t rows = std::min<int64_t>(n, int64_t(1) << 27);
+        const int64_t rows = std::min<int64_t>((n + 1) / 2, int64_t(1) << 28);
         const int64_t cell = (rows + rows / 4) / (parts * ctas) + 64;
         const int vbytes = a.vals ? type_size(gb->val_type) : 0;
         int32_t rc = gb_spill_reserve(gb, static_cast<uint64_t>(parts * ctas * cell), vbytes, parts * ctas, s);

@@ -36,7 +36,8 @@ constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsume
 constexpr int kQueueCap = 64;                              // per-warp queue of rows for the global table
 constexpr int kSpillThreads = 512;                         // threads of a spill-pass CTA
 constexpr int kSeenWords = 1024;                           // 32768-bit filter of keys seen once (spilling tables)
-constexpr int kDecideTile = 3;                             // tile index at which a warp judges its hit rate
+constexpr int kCountTile = 4;                              // from this tile on a warp counts its shared-table hits
+constexpr int kDecideTile = 12;                            // tile index at which a warp judges its hit rate
 constexpr uint32_t kMaxWaitIters = 1u << 18;               // bounded mbarrier waits (seconds, then give up)
 
 // `col OP constant` as an interval of the column type: keep = (lo <= x && x <= hi) != invert.
@@ -845,6 +846,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
 
         bool use_smem = S > 0;
         unsigned my_hits = 0, my_tries = 0;
+        bool spill_ok = spill_on;  // cleared, with use_smem, when this warp's shared-table hit rate is low
         const int smem_shift = 32 - (31 - __clz(S > 0 ? S : 1));
         // Per-warp queue of rows for the global table (raw rows: key word, value bits, kind | agg flag).
         uint64_t* qkw = reinterpret_cast<uint64_t*>(sm + a.so_queue) + warp * kQueueCap;
@@ -958,10 +960,8 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 const uint32_t h = bucket_home(kw, smem_shift);
                 bool found = false;
                 slot_s = s_find(tab.key, S, a.probe, kw, h, &found);
-                if (!spill_on) {
-                    ++my_tries;
-                    my_hits += found ? 1u : 0u;
-                }
+                ++my_tries;
+                my_hits += slot_s >= 0 ? 1u : 0u;
             } else {
                 slot_s = S + (kind == KK_ESCAPE ? 1 : 0);
                 if (*reinterpret_cast<volatile uint64_t*>(&tab.key[slot_s]) == kEmpty)
@@ -971,7 +971,7 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 if (agg_it) s_add<VT>(tab, a, slot_s, v, qv, has_vals);
                 return false;
             }
-            if (spill_on && kind == KK_NORMAL && agg_it) meta_out |= 8u;  // the queue drain spills it
+            if (spill_ok && kind == KK_NORMAL && agg_it) meta_out |= 8u;  // the queue drain spills it
             return true;
         };
         // Queues row (kw, v, meta) of a lane whose `miss` is set; drains 32 rows when the queue is nearly full.
@@ -1026,15 +1026,13 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                     bool found = false;
                     slot = s_find32(tab.ak, S, a.probe, kw, h0, &found);
                     hit = slot >= 0;
-                    if (!spill_on) {
-                        ++my_tries;
-                        my_hits += found ? 1u : 0u;
-                    }
                 }
             }
+            my_tries += ok ? 1u : 0u;
+            my_hits += hit ? 1u : 0u;
             if (hit) s_add<VT>(tab, a, slot, v, qv, has_vals);
             const bool miss = act && !hit;
-            const uint32_t spillable = (spill_on && normal && inwin) ? 8u : 0u;
+            const uint32_t spillable = (spill_ok && normal && inwin) ? 8u : 0u;
             enqueue(miss, kw, v, static_cast<uint32_t>(normal ? KK_NORMAL : KK_ESCAPE) | 4u | spillable);
         };
         int s = 0;
@@ -1144,9 +1142,15 @@ __global__ void __launch_bounds__(kAggThreads, 1) gb_agg_kernel(const AggArgs a)
                 drain32(qn);
                 __syncwarp();
             }
-            if (q == kDecideTile && use_smem && !spill_on) {
+            // After the table's fill phase a warp judges its shared-table hit rate.  Below 1/2 (keys spread evenly
+            // over many more groups than the table holds) the spill would carry most rows through HBM twice and
+            // through the spill pass, which measured slower than inserting them into the global table directly:
+            // misses go to the global table.  Below 1/8 the warp also stops probing the shared table.
+            if (q + 1 == kCountTile) my_hits = my_tries = 0;
+            if (q == kDecideTile && use_smem) {
                 const unsigned hits = __reduce_add_sync(0xffffffffu, my_hits);
                 const unsigned tries = __reduce_add_sync(0xffffffffu, my_tries);
+                if (tries >= 256 && hits * 2u < tries) spill_ok = false;
                 if (tries >= 256 && hits * 8u < tries) use_smem = false;
             }
             if (++s == a.NS) {
