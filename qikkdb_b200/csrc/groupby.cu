@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
 #include <vector>
 
 #include "groupby_agg.cuh"
@@ -96,26 +97,78 @@ static int32_t launch_spill(const qdb_gb* gb, const AggArgs& a, size_t smem, int
     }
 }
 
-// The table's spill area (kept across calls, grown on demand): rows key words, rows values of vbytes bytes,
-// and the fill counts of `cells` cells.
-static int32_t gb_spill_reserve(qdb_gb* gb, uint64_t rows, int vbytes, int64_t cells, cudaStream_t s) {
-    if (gb->spill_rows >= rows && gb->spill_vbytes >= vbytes && gb->spill_cells >= cells) return QDB_OK;
-    dev_free(gb->spill_keys, s);
-    dev_free(gb->spill_vals, s);
-    dev_free(gb->spill_fill, s);
-    gb->spill_keys = nullptr;
-    gb->spill_vals = nullptr;
-    gb->spill_fill = nullptr;
-    gb->spill_rows = 0;
-    gb->spill_cells = 0;
-    int32_t rc = dev_alloc(reinterpret_cast<void**>(&gb->spill_fill), static_cast<size_t>(cells) * sizeof(uint32_t), s);
-    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&gb->spill_keys), rows * 8, s);
-    if (rc == QDB_OK && vbytes) rc = dev_alloc(&gb->spill_vals, rows * static_cast<uint64_t>(vbytes), s);
-    if (rc != QDB_OK) return rc;
-    gb->spill_rows = rows;
-    gb->spill_vbytes = vbytes;
-    gb->spill_cells = cells;
+// The spill area of the aggregation pass: one per device, shared by every table and kept for the life of the
+// process (grown on demand), because the reference's dispatcher creates a table per query and a multi-GB area
+// allocated per table would grow the memory pool on every query.  A call borrows the area only while it enqueues
+// its two launches; an event recorded after them on the call's stream orders the next borrower (on any stream)
+// after them on the GPU.
+namespace {
+struct SpillArea {
+    std::mutex mu;
+    uint64_t* keys = nullptr;
+    void* vals = nullptr;
+    uint32_t* fill = nullptr;
+    uint64_t rows = 0;
+    int64_t cells = 0;
+    int32_t vbytes = 0;
+    cudaEvent_t done = nullptr;  // recorded after the last call that used the area
+};
+SpillArea g_spill[64];
+}  // namespace
+
+// Locks the device's spill area and makes it at least rows x (8 + vbytes) bytes with `cells` fill counters,
+// ordered on stream s after every earlier use.  The caller fills *area and must call spill_release.
+static int32_t spill_acquire(int dev, uint64_t rows, int vbytes, int64_t cells, cudaStream_t s, SpillArea** out) {
+    if (dev < 0 || dev >= 64) return fail(QDB_ERR_INVALID, "spill area: device index out of range");
+    SpillArea& A = g_spill[dev];
+    A.mu.lock();
+    if (!A.done && cudaEventCreateWithFlags(&A.done, cudaEventDisableTiming) != cudaSuccess) {
+        A.mu.unlock();
+        return cuda_fail(cudaGetLastError(), "cudaEventCreate(spill area)");
+    }
+    if (A.rows > 0) {
+        const cudaError_t e = cudaStreamWaitEvent(s, A.done, 0);
+        if (e != cudaSuccess) {
+            A.mu.unlock();
+            return cuda_fail(e, "cudaStreamWaitEvent(spill area)");
+        }
+    }
+    if (A.rows < rows || A.vbytes < vbytes || A.cells < cells) {
+        dev_free(A.keys, s);
+        dev_free(A.vals, s);
+        dev_free(A.fill, s);
+        A.keys = nullptr;
+        A.vals = nullptr;
+        A.fill = nullptr;
+        A.rows = 0;
+        A.cells = 0;
+        A.vbytes = 0;
+        const uint64_t r = std::max<uint64_t>(rows, A.rows);
+        int32_t rc = dev_alloc(reinterpret_cast<void**>(&A.fill), static_cast<size_t>(cells) * sizeof(uint32_t), s);
+        if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&A.keys), r * 8, s);
+        if (rc == QDB_OK && vbytes) rc = dev_alloc(&A.vals, r * static_cast<uint64_t>(vbytes), s);
+        if (rc != QDB_OK) {
+            dev_free(A.keys, s);
+            dev_free(A.vals, s);
+            dev_free(A.fill, s);
+            A.keys = nullptr;
+            A.vals = nullptr;
+            A.fill = nullptr;
+            A.mu.unlock();
+            return rc;
+        }
+        A.rows = r;
+        A.cells = cells;
+        A.vbytes = vbytes;
+    }
+    *out = &A;
     return QDB_OK;
+}
+
+// Records the end of this call's use of the area on stream s and unlocks it.
+static void spill_release(SpillArea* A, cudaStream_t s) {
+    cudaEventRecord(A->done, s);
+    A->mu.unlock();
 }
 
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -302,9 +355,6 @@ int32_t qdb_gb_destroy(qdb_gb* gb) {
     dev_free(gb->main.slots, 0);
     dev_free(gb->aux.slots, 0);
     dev_free(gb->counters, 0);
-    dev_free(gb->spill_keys, 0);
-    dev_free(gb->spill_vals, 0);
-    dev_free(gb->spill_fill, 0);
     if (prev != gb->device) cudaSetDevice(prev);
     delete gb;
     return QDB_OK;
@@ -500,6 +550,7 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
             spill_bits = -1;
         }
     }
+    SpillArea* spill = nullptr;
     if (spill_bits >= 0) {
         // Spill area: one cell per (partition, CTA).  A cell holds 5/4 of its share of half this call's rows (at
         // most 2^28 rows in all) plus 64: warps whose shared-table hit rate is below 1/2 stop spilling, so hashed
@@ -510,11 +561,11 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
         const int64_t rows = std::min<int64_t>((n + 1) / 2, int64_t(1) << 28);
         const int64_t cell = (rows + rows / 4) / (parts * ctas) + 64;
         const int vbytes = a.vals ? type_size(gb->val_type) : 0;
-        int32_t rc = gb_spill_reserve(gb, static_cast<uint64_t>(parts * ctas * cell), vbytes, parts * ctas, s);
+        int32_t rc = spill_acquire(gb->device, static_cast<uint64_t>(parts * ctas * cell), vbytes, parts * ctas, s, &spill);
         if (rc != QDB_OK) return rc;
-        a.spill_keys = gb->spill_keys;
-        a.spill_vals = vbytes ? gb->spill_vals : nullptr;
-        a.spill_fill = gb->spill_fill;
+        a.spill_keys = spill->keys;
+        a.spill_vals = vbytes ? spill->vals : nullptr;
+        a.spill_fill = spill->fill;
         a.spill_cell = cell;
         a.spill_bits = spill_bits;
         a.spill_ctas = static_cast<int32_t>(ctas);
@@ -526,7 +577,10 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     a.so_stage = static_cast<int32_t>(a.so_spill + spill_words_bytes);
     const size_t smem = a.so_stage + stage_area;
     int32_t rc = launch_agg(gb, a, ptype, nulls, smem, s);
-    if (rc != QDB_OK || spill_bits < 0) return rc;
+    if (rc != QDB_OK || spill_bits < 0) {
+        if (spill) spill_release(spill, s);
+        return rc;
+    }
 
     // Spill pass: partitions x slices CTAs, each with a shared table of S2spill slots.
     AggArgs b = a;
@@ -535,7 +589,9 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     const size_t smem2 = layout_table(b, S2spill);
     const int64_t parts = int64_t(1) << spill_bits;
     const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, (2 * di.sm_count + parts - 1) / parts));
-    return launch_spill(gb, b, smem2, parts * slices, s);
+    rc = launch_spill(gb, b, smem2, parts * slices, s);
+    spill_release(spill, s);
+    return rc;
 }
 
 

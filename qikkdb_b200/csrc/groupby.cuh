@@ -92,13 +92,6 @@ struct qdb_gb {
     qdb::Region aux;       // composite keys with a NULL component (allocated on first use)
     unsigned long long* counters = nullptr;  // [0] groups claimed, [1] status word (int32 in low half)
     int64_t last_hint_rows = 0;
-    // spill area of the aggregation pass (allocated on first use, grown on demand)
-    uint64_t* spill_keys = nullptr;
-    void* spill_vals = nullptr;
-    uint32_t* spill_fill = nullptr;
-    uint64_t spill_rows = 0;
-    int64_t spill_cells = 0;
-    int32_t spill_vbytes = 0;
 };
 
 namespace qdb {
