@@ -512,7 +512,7 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     int spill_bits = -1;
     int S2spill = 0;
     if (smem_place && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
-        const size_t budget2 = 100 * 1024;  // two spill-pass CTAs per SM
+        const size_t budget2 = static_cast<size_t>(env_int("QDB_SPILL_SMEM_KB", 50)) * 1024;  // 50 KB: four spill-pass CTAs per SM
         int S2 = 1 << 15;
         while (S2 >= 256 && static_cast<size_t>(S2 + 2) * bps + 256 > budget2) S2 >>= 1;
         if (S2 >= 256) {
@@ -588,7 +588,7 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     b.probe = 64;
     const size_t smem2 = layout_table(b, S2spill);
     const int64_t parts = int64_t(1) << spill_bits;
-    const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, (2 * di.sm_count + parts - 1) / parts));
+    const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, (4 * di.sm_count + parts - 1) / parts));
     rc = launch_spill(gb, b, smem2, parts * slices, s);
     spill_release(spill, s);
     return rc;
