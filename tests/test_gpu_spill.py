@@ -75,3 +75,39 @@ def test_negative_float_sums(cuda):
     v = (rng.random(n) * 2000.0 - 1000.0).astype(np.float32)
     rel, _, _ = run_both(k, v, ["sum", "avg", "count", "min", "max"], 128, 0, val_is_float=True)
     assert rel <= FLOAT_RTOL
+
+
+def test_tables_on_two_streams_share_the_spill_area(cuda):
+    """Two spilling tables fed alternately on two streams: the per-device spill area is ordered between the calls
+    by its event, so both results equal the oracle's."""
+    import torch
+
+    import oracle
+    from gpu_compare import compare
+    from qikkdb_b200.groupby import GroupByTable
+
+    n = 1 << 21
+    cols = []
+    for seed in (91, 92):
+        k = dg.zipf_i64(seed, 0, n, 200_000, 1.05)
+        v = dg.lognormal_f32(seed, 1, n, 1.0, 1.0)
+        cols.append((k, v))
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    tables = [GroupByTable(["sum", "count", "max"], np.int64, np.float32, 1 << 18, stream=s.cuda_stream)
+              for s in streams]
+    blocks = 8
+    bounds = np.linspace(0, n, blocks + 1).astype(np.int64)
+    dev = []
+    for (k, v), s in zip(cols, streams):
+        with torch.cuda.stream(s):
+            dev.append((torch.from_numpy(k).cuda(), torch.from_numpy(v).cuda()))
+    torch.cuda.synchronize()
+    for b0, b1 in zip(bounds[:-1], bounds[1:]):
+        for t, (dk, dv), s in zip(tables, dev, streams):
+            t.process([dk[b0:b1]], dv[b0:b1], int(b1 - b0), stream=s.cuda_stream, sync=False)
+    for t, s in zip(tables, streams):
+        s.synchronize()
+        t.check(stream=s.cuda_stream)
+    for t, (k, v) in zip(tables, cols):
+        rel = compare(t.results_numpy(), oracle.groupby(k, v), ["sum", "count", "max"], True)
+        assert rel <= FLOAT_RTOL
