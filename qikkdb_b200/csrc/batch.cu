@@ -405,6 +405,8 @@ static int32_t check_cfg(const qdb_gb_batch* b, const qdb_gb_query& q, const qdb
     if (c.rows_per_thread != 1 && c.rows_per_thread != 2 && c.rows_per_thread != 4)
         return fail(QDB_ERR_INVALID, "batch cfg: rows_per_thread must be 1, 2 or 4");
     if (c.chunk_rows < 64 || c.chunk_rows % 64) return fail(QDB_ERR_INVALID, "batch cfg: chunk_rows must be a positive multiple of 64");
+    // an item's shared float sums are 64-bit fixed-point words with addends below 2^39
+    if (c.chunk_rows > (int64_t(1) << 24)) return fail(QDB_ERR_INVALID, "batch cfg: chunk_rows must be at most 2^24");
     if (c.placement == QDB_PLACE_SHARED) {
         const int S = c.smem_slots;
         if (S < 64 || (S % 32)) return fail(QDB_ERR_INVALID, "batch cfg: smem_slots must be a multiple of 32, >= 64");

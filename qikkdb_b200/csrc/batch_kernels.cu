@@ -83,19 +83,55 @@ struct BSmem {
     unsigned int* cnt;
 };
 
+// float SUM in a shared slot: a 64-bit two's-complement fixed-point accumulator of q = v * 2^F in the slot's sum
+// word, F = 31 - e with e the largest exponent (|v| < 2^e) of the item's first tile.  A value is kept when its
+// shift e_v - sh0 lies in [-4, 15], so q is in [2^19, 2^39): at least 20 significant bits (rounded when the shift is
+// negative), and the at most 2^24 rows of an item cannot overflow the word.  Other values (and NaN, Inf,
+// subnormals) take the global FP64 path.
+struct BFix {
+    int sh0 = 119;     // emax + 119
+    double inv = 0.0;  // 2^-F
+};
+
+__device__ __forceinline__ BFix b_fix(int emax) {
+    emax = max(-100, min(100, emax));
+    BFix f;
+    f.sh0 = emax + 119;
+    f.inv = ldexp(1.0, emax - 31);
+    return f;
+}
+
+__device__ __forceinline__ long long b_addend(float v, const BFix& f, bool* ok) {
+    const uint32_t b = __float_as_uint(v);
+    const int e = static_cast<int>((b >> 23) & 0xffu);
+    const uint32_t fr = b & 0x7fffffu;
+    if (e == 0) {
+        *ok = fr == 0u;
+        return 0ll;
+    }
+    const int sh = e - f.sh0;
+    *ok = e != 0xff && sh >= -4 && sh <= 15;
+    if (!*ok) return 0ll;
+    const uint32_t m = fr | 0x800000u;
+    const long long q = sh >= 0 ? static_cast<long long>(static_cast<uint64_t>(m) << sh)
+                                : static_cast<long long>((m + (1u << (-sh - 1))) >> (-sh));
+    return (b >> 31) ? -q : q;
+}
+
+// q: the integer value, or the fixed-point addend of a float value.
 template <typename VT>
-__device__ __forceinline__ void b_s_acc(const BSmem& t, int s, VT v, bool has_vals, bool has_sum, bool has_min,
-                                        bool has_max) {
+__device__ __forceinline__ void b_s_acc(const BSmem& t, int s, VT v, long long q, bool has_vals, bool has_sum,
+                                        bool has_min, bool has_max) {
     atomicAdd(t.cnt + s, 1u);
     if (!has_vals) return;
     if (has_sum) {
-        if constexpr (std::is_floating_point<VT>::value) {
-            atomicAdd(reinterpret_cast<double*>(t.sum) + s, static_cast<double>(v));
+        if constexpr (std::is_same<VT, double>::value) {
+            atomicAdd(reinterpret_cast<double*>(t.sum) + s, v);
         } else {
             // The 64-bit two's-complement add as two 32-bit shared atomics on the halves of the word (the carry out
             // of the low half is read from the value its atomic returns): the same word as a 64-bit atomicAdd,
             // without the 64-bit CAS loop that serialises when many lanes hit one slot.
-            const unsigned long long u = static_cast<unsigned long long>(static_cast<long long>(v));
+            const unsigned long long u = static_cast<unsigned long long>(q);
             unsigned* w = reinterpret_cast<unsigned*>(t.sum + s);
             const unsigned x0 = static_cast<unsigned>(u), x1 = static_cast<unsigned>(u >> 32);
             const unsigned old = atomicAdd(w, x0);
@@ -173,6 +209,8 @@ struct BGroupSmem {
     uint64_t csync;
     uint64_t pad;
     BStageMeta meta[kBStages];
+    int32_t emax;  // largest value exponent of the current item's first tile (float values)
+    int32_t pad2;
 };
 static_assert(sizeof(BGroupSmem) <= kBHeaderBytes, "group header");
 
@@ -235,7 +273,8 @@ __device__ void b_clear(unsigned char* base, const BInst& I, int ctid, int cthre
 
 // Merges one query's shared tables into its global table.
 template <typename VT>
-__device__ void b_flush(unsigned char* base, const BInst& I, int ctid, int cthreads, unsigned long long* claims) {
+__device__ void b_flush(unsigned char* base, const BInst& I, int ctid, int cthreads, unsigned long long* claims,
+                        const BFix& fx) {
     constexpr bool V32 = sizeof(VT) == 4;
     const int RS = I.S * I.R;
     if (RS == 0) return;
@@ -251,7 +290,11 @@ __device__ void b_flush(unsigned char* base, const BInst& I, int ctid, int cthre
         uint64_t* slot = g_find(main, L.W, key, mix64(key), I.counters, claims);
         if (!slot) continue;
         const unsigned long long c = t.cnt[i];
-        const uint64_t sumbits = has_sum ? t.sum[i] : 0ull;
+        uint64_t sumbits = has_sum ? t.sum[i] : 0ull;
+        if (has_sum && std::is_same<VT, float>::value) {  // fixed point -> FP64
+            const double d = static_cast<double>(static_cast<long long>(sumbits)) * fx.inv;
+            memcpy(&sumbits, &d, 8);
+        }
         long long mn = 0, mx = 0;
         if (has_mm) {
             if (V32) {
@@ -297,7 +340,8 @@ constexpr int kProbeRounds = 4;
 // sequence rather than the sum of them.
 template <typename VT, int RPT>
 __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int voff, int poff, int nrows,
-                       unsigned char* tbase, int wig, int cw, uint16_t* list, unsigned long long* claims) {
+                       unsigned char* tbase, int wig, int cw, uint16_t* list, unsigned long long* claims,
+                       const BFix& fx) {
     constexpr bool V32 = sizeof(VT) == 4;
     const int lane = threadIdx.x & 31;
     const int per_warp = (((nrows + cw - 1) / cw) + 31) & ~31;
@@ -379,9 +423,16 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
 #pragma unroll
             for (int u = 0; u < RPT; ++u) {
                 if (!ok[u]) continue;
-                const int s = (kw[u] != kEmpty) ? b_s_find(t.key, S, probe, kw[u]) : -1;
+                bool inwin = true;
+                long long q = 0;
+                if constexpr (std::is_same<VT, float>::value) {
+                    if (has_sum) q = b_addend(v[u], fx, &inwin);
+                } else if constexpr (!std::is_floating_point<VT>::value) {
+                    q = static_cast<long long>(v[u]);
+                }
+                const int s = (kw[u] != kEmpty && inwin) ? b_s_find(t.key, S, probe, kw[u]) : -1;
                 if (s >= 0) {
-                    b_s_acc<VT>(t, s, v[u], has_vals, has_sum, has_min, has_max);
+                    b_s_acc<VT>(t, s, v[u], q, has_vals, has_sum, has_min, has_max);
                 } else {
                     uint64_t* slot = (kw[u] == kEmpty) ? g_special(main, W, 1, claims)
                                                        : g_find(main, W, kw[u], mix64(kw[u]), I.counters, claims);
@@ -442,12 +493,13 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
 template <typename VT>
 __device__ __forceinline__ void b_members_tile(const BGroup& grp, const BInst* desc, const unsigned char* st,
                                                int koff, int voff, int poff, int nrows, unsigned char* tbase,
-                                               int wig, int cw, uint16_t* list, int rpt, unsigned long long* claims) {
+                                               int wig, int cw, uint16_t* list, int rpt, unsigned long long* claims,
+                                               const BFix& fx) {
     for (int k = 0; k < grp.n_members; ++k) {
         switch (rpt) {
-            case 1: b_tile<VT, 1>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
-            case 2: b_tile<VT, 2>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
-            default: b_tile<VT, 4>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k); break;
+            case 1: b_tile<VT, 1>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k, fx); break;
+            case 2: b_tile<VT, 2>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k, fx); break;
+            default: b_tile<VT, 4>(desc[k], st, koff, voff, poff, nrows, tbase, wig, cw, list, claims + k, fx); break;
         }
     }
 }
@@ -460,8 +512,8 @@ __device__ __forceinline__ void b_members_clear(const BGroup& grp, const BInst* 
 
 template <typename VT>
 __device__ __forceinline__ void b_members_flush(const BGroup& grp, const BInst* desc, unsigned char* tbase, int ctid,
-                                                int cthreads, unsigned long long* claims) {
-    for (int k = 0; k < grp.n_members; ++k) b_flush<VT>(tbase, desc[k], ctid, cthreads, claims + k);
+                                                int cthreads, unsigned long long* claims, const BFix& fx) {
+    for (int k = 0; k < grp.n_members; ++k) b_flush<VT>(tbase, desc[k], ctid, cthreads, claims + k, fx);
 }
 
 // Copies the rows of [r, r + nrows) of one column that a bulk copy cannot move (the final < 16 bytes of an
@@ -583,6 +635,7 @@ __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchA
             unsigned long long* claims = s_claims[g];
             uint32_t seq = 0, cpar = 0;
             unsigned long long t0 = 0;
+            BFix fx;  // the current item's fixed-point scale (float values)
             for (;;) {
                 const int s = static_cast<int>(seq % kBStages);
                 if (!b_wait(&h->full[s], (seq / kBStages) & 1u, err)) break;
@@ -602,6 +655,7 @@ __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchA
                     for (int w = ctid; w < grp.n_members * kWords; w += cthreads)
                         reinterpret_cast<uint64_t*>(desc)[w] =
                             reinterpret_cast<const uint64_t*>(ba.inst + grp.members[w / kWords])[w % kWords];
+                    if (ctid == 0) h->emax = INT_MIN;
                     b_csync(&h->csync, cpar, err);
                     switch (vk) {
                         case VK_I64: b_members_clear<int64_t>(grp, desc, tbase, ctid, cthreads); break;
@@ -609,24 +663,36 @@ __global__ void __launch_bounds__(kBThreads, 1) gb_batch_agg_kernel(const BatchA
                         case VK_F64: b_members_clear<double>(grp, desc, tbase, ctid, cthreads); break;
                         default: b_members_clear<int32_t>(grp, desc, tbase, ctid, cthreads); break;
                     }
+                    if (vk == VK_F32) {  // the fixed-point scale of this item's float sums
+                        int e = INT_MIN;
+                        const float* vals = reinterpret_cast<const float*>(st + voff);
+                        for (int j = ctid; j < m.nrows; j += cthreads) {
+                            const uint32_t b = __float_as_uint(vals[j]);
+                            const int be = static_cast<int>((b >> 23) & 0xffu);
+                            if (be != 0 && be != 0xff) e = max(e, be - 126);
+                        }
+                        e = __reduce_max_sync(0xffffffffu, e);
+                        if (lane == 0 && e != INT_MIN) atomicMax(&h->emax, e);
+                    }
                     b_csync(&h->csync, cpar, err);
+                    fx = b_fix(h->emax == INT_MIN ? 0 : h->emax);
                 }
                 const int rpt = grp.rpt;
                 switch (vk) {
-                    case VK_I64: b_members_tile<int64_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
-                    case VK_F32: b_members_tile<float>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
-                    case VK_F64: b_members_tile<double>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
-                    default: b_members_tile<int32_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims); break;
+                    case VK_I64: b_members_tile<int64_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims, fx); break;
+                    case VK_F32: b_members_tile<float>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims, fx); break;
+                    case VK_F64: b_members_tile<double>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims, fx); break;
+                    default: b_members_tile<int32_t>(grp, desc, st, koff, voff, poff, m.nrows, tbase, wig, cw, s_list[warp], rpt, claims, fx); break;
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&h->empty[s]);
                 if (m.flags & kMetaLast) {
                     b_csync(&h->csync, cpar, err);
                     switch (vk) {
-                        case VK_I64: b_members_flush<int64_t>(grp, desc, tbase, ctid, cthreads, claims); break;
-                        case VK_F32: b_members_flush<float>(grp, desc, tbase, ctid, cthreads, claims); break;
-                        case VK_F64: b_members_flush<double>(grp, desc, tbase, ctid, cthreads, claims); break;
-                        default: b_members_flush<int32_t>(grp, desc, tbase, ctid, cthreads, claims); break;
+                        case VK_I64: b_members_flush<int64_t>(grp, desc, tbase, ctid, cthreads, claims, fx); break;
+                        case VK_F32: b_members_flush<float>(grp, desc, tbase, ctid, cthreads, claims, fx); break;
+                        case VK_F64: b_members_flush<double>(grp, desc, tbase, ctid, cthreads, claims, fx); break;
+                        default: b_members_flush<int32_t>(grp, desc, tbase, ctid, cthreads, claims, fx); break;
                     }
                     b_csync(&h->csync, cpar, err);
                     if (ctid == 0) {
