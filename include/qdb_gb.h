@@ -140,7 +140,9 @@ int32_t qdb_gb_group_count(qdb_gb* gb, int64_t* out, void* stream);
  * fused filter; `mask` (optional) is a precomputed int8 filter mask (non-zero = keep).  Both may be
  * given; a row is aggregated when it passes both.  Errors raised by the kernel (HASH_TABLE_FULL) are
  * latched in the table and returned by qdb_gb_check (the ErrorFlagSwapper::Swap step,
- * qikkDB/QueryEngine/GPUCore/ErrorFlagSwapper.h:32-50). */
+ * qikkDB/QueryEngine/GPUCore/ErrorFlagSwapper.h:32-50).  A table whose max_groups exceeds one shared-memory
+ * table (and placement is not QDB_PLACE_GLOBAL) uses the device's spill area, allocated by the first call that
+ * needs it and kept, grown on demand, until the process exits. */
 int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
                        const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
                        const int8_t* mask, void* stream);
