@@ -85,8 +85,8 @@ struct BSmem {
 
 // float SUM in a shared slot: a 64-bit two's-complement fixed-point accumulator of q = v * 2^F in the slot's sum
 // word, F = 31 - e with e the largest exponent (|v| < 2^e) of the item's first tile.  A value is kept when its
-// shift e_v - sh0 lies in [-4, 15], so q is in [2^19, 2^39): at least 20 significant bits (rounded when the shift is
-// negative), and the at most 2^24 rows of an item cannot overflow the word.  Other values (and NaN, Inf,
+// shift e_v - sh0 lies in [-1, 15], so q is in [2^22, 2^39): exact, or rounded to 23 significant bits when the
+// shift is -1, and the at most 2^24 rows of an item cannot overflow the word.  Other values (and NaN, Inf,
 // subnormals) take the global FP64 path.
 struct BFix {
     int sh0 = 119;     // emax + 119
@@ -110,7 +110,7 @@ __device__ __forceinline__ long long b_addend(float v, const BFix& f, bool* ok) 
         return 0ll;
     }
     const int sh = e - f.sh0;
-    *ok = e != 0xff && sh >= -4 && sh <= 15;
+    *ok = e != 0xff && sh >= -1 && sh <= 15;
     if (!*ok) return 0ll;
     const uint32_t m = fr | 0x800000u;
     const long long q = sh >= 0 ? static_cast<long long>(static_cast<uint64_t>(m) << sh)

@@ -337,3 +337,34 @@ def test_batch_shared_scan(cuda, share):
     assert (status == 0).all()
     for s, r in zip(specs, b.results_all()):
         s.check(r)
+
+
+def test_batch_float_sums_outside_fixed_point_window(cuda):
+    """Shared-table float sums are fixed point per work item, scaled from the item's first tile: values far from
+    those magnitudes (lognormal with sigma 10, some negative, zeros) take the FP64 global path, and every sum stays
+    within tolerance of the FP64 oracle; a chunk above 2^24 rows is rejected."""
+    specs = []
+    for i, (n, card) in enumerate([(400_000, 50), (300_000, 900)]):
+        s = Spec(400 + i, np.int32, np.float32, n, card, ["sum", "avg", "min", "max", "count"])
+        v = dg.lognormal_f32(400 + i, 5, n, 0.0, 10.0)
+        v[::11] *= -1.0
+        v[::7] = 0.0
+        s.v = v
+        s.dv = _dev(v)
+        s.ref = oracle.groupby(s.k, v)
+        specs.append(s)
+    b = GroupByBatch(len(specs), 1 << 28, 1 << 26)
+    b.set([s.query() for s in specs])
+    for i, s in enumerate(specs):
+        slots = 64
+        while slots < 2 * (s.max_groups + 1):
+            slots *= 2
+        b.set_cfg(i, placement=capi.QDB_PLACE_SHARED, replicas=1, warps=12, rows_per_thread=2, chunk_rows=65536,
+                  smem_slots=min(slots, 2048))
+    with pytest.raises(QueryEngineError):
+        b.set_cfg(0, chunk_rows=(1 << 24) + 64)
+    b.run()
+    _, status = b.fetch()
+    assert (status == 0).all()
+    for s, r in zip(specs, b.results_all()):
+        s.check(r)
