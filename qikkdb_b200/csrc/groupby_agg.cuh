@@ -33,7 +33,7 @@ constexpr int kConsumerWarps = 16;
 constexpr int kConsumerThreads = kConsumerWarps * 32;     // 512
 constexpr int kAggThreads = kConsumerThreads + 32;         // + one producer warp: 544 threads
 constexpr int kRowsPerWarpUnit = 64;                       // a tile is kConsumerWarps * R rows, R a multiple of 64
-constexpr int kQueueCap = 64;                              // per-warp queue of rows for the global table
+constexpr int kQueueCap = 64;                              // per-warp queue of shared-table misses
 constexpr int kSpillThreads = 512;                         // threads of a spill-pass CTA
 constexpr int kSeenWords = 1024;                           // 32768-bit filter of keys seen once (spilling tables)
 constexpr int kCountTile = 4;                              // from this tile on a warp counts its shared-table hits
@@ -506,13 +506,10 @@ __device__ __forceinline__ long long sum_addend(VT v, const FixScale& f, bool* o
         const uint32_t b = __float_as_uint(v);
         const int e = static_cast<int>((b >> 23) & 0xffu);
         const uint32_t fr = b & 0x7fffffu;
-        if (e == 0) {
-            *ok = fr == 0u;  // zero is exact; subnormals take the FP64 path
-            return 0ll;
-        }
         const int sh = e - f.sh0;
-        *ok = e != 0xff && sh >= 1 && sh <= 39;
-        const long long q = *ok ? static_cast<long long>(static_cast<uint64_t>(fr | 0x800000u) << sh) : 0ll;
+        const bool inw = e != 0 && e != 0xff && sh >= 1 && sh <= 39;
+        *ok = inw || (b & 0x7fffffffu) == 0u;  // zero is exact; subnormals, NaN and Inf take the FP64 path
+        const long long q = inw ? static_cast<long long>(static_cast<uint64_t>(fr | 0x800000u) << sh) : 0ll;
         return (b >> 31) ? -q : q;
     } else if constexpr (std::is_floating_point<VT>::value) {
         const double d = static_cast<double>(v);
