@@ -7,7 +7,7 @@
 #include <mutex>
 #include <vector>
 
-#include "groupby_agg.cuh"
+#include "groupby_fast.cuh"
 
 namespace qdb {
 
@@ -93,6 +93,30 @@ static int32_t launch_spill(const qdb_gb* gb, const AggArgs& a, size_t smem, int
         case VK_I64: return launch_spill_t<int64_t>(a, smem, grid, st);
         case VK_F32: return launch_spill_t<float>(a, smem, grid, st);
         case VK_F64: return launch_spill_t<double>(a, smem, grid, st);
+        default: return fail(QDB_ERR_INVALID, "unsupported value type");
+    }
+}
+
+static int32_t launch_fast(const qdb_gb* gb, const AggArgs& a, int32_t ptype, size_t smem, cudaStream_t st) {
+    const ValKind vk = val_kind(gb->val_type);
+    if (gb->n_key_cols == 2) return launch_fast_comp(a, vk, ptype, smem, st);
+    switch (gb->key_type) {
+        case QDB_INT32: return launch_fast_i32(a, vk, ptype, smem, st);
+        case QDB_INT64: return launch_fast_i64(a, vk, ptype, smem, st);
+        case QDB_FLOAT: return launch_fast_f32(a, vk, ptype, smem, st);
+        case QDB_DOUBLE: return launch_fast_f64(a, vk, ptype, smem, st);
+        default: return fail(QDB_ERR_INVALID, "unsupported key type");
+    }
+}
+
+static int32_t launch_fspill(const qdb_gb* gb, const AggArgs& a, size_t smem, int64_t grid, int32_t slices,
+                             cudaStream_t st) {
+    if (fast_mode(a) == 0) return launch_fspill_t<int32_t, 0>(a, smem, grid, slices, st);
+    switch (val_kind(gb->val_type)) {
+        case VK_I32: return launch_fspill_m<int32_t>(a, smem, grid, slices, st);
+        case VK_I64: return launch_fspill_m<int64_t>(a, smem, grid, slices, st);
+        case VK_F32: return launch_fspill_m<float>(a, smem, grid, slices, st);
+        case VK_F64: return launch_fspill_m<double>(a, smem, grid, slices, st);
         default: return fail(QDB_ERR_INVALID, "unsupported value type");
     }
 }
@@ -296,6 +320,151 @@ PredInterval pred_interval(const qdb_pred& p) {
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Plan and launch of the fast pass (groupby_fast.cuh) for a call without NULL masks or a precomputed mask whose
+// columns are 16-byte aligned and hold at least one whole tile.  *used is false when the plan does not fit shared
+// memory (the caller then takes the general pass).
+// ---------------------------------------------------------------------------------------------
+static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t ptype, cudaStream_t s, bool* used) {
+    *used = false;
+    const DeviceInfo& di = device_info();
+    const ValKind vk = val_kind(gb->val_type);
+    // A table whose aggregates never read the values (COUNT only, no NULL masks here) streams the keys alone.
+    if (fast_mode(a) == 0) a.vals = nullptr;
+    const int ks = (gb->n_key_cols == 2) ? 4 : type_size(gb->key_type);
+    const int vs = a.vals ? type_size(gb->val_type) : 0;
+    const int ps = a.pcol ? type_size(pred->type) : 0;
+    const int row_bytes = ks * gb->n_key_cols + vs + ps;
+    // Stages: enough bytes in flight to cover the HBM latency at an SM's share of the bandwidth (about 48 KB), and at
+    // least three when they fit (a warp may hold two stages while it carries rows over).
+    const int stage_bytes = kFastT * row_bytes;
+    int NS = static_cast<int>(env_int("QDB_FAST_STAGES", stage_bytes <= 16 * 1024 ? 4 : (stage_bytes <= 40 * 1024 ? 3 : 2)));
+    NS = std::min(6, std::max(2, NS));
+    const size_t ring = static_cast<size_t>(NS) * stage_bytes;
+    if (ring > 128 * 1024) return QDB_OK;
+    // Ring columns: stage s, row i of column c at off_c + (s T + i) * size_c.
+    StageLayout sl;
+    int32_t off = 0;
+    sl.key0 = off;
+    off += NS * kFastT * ks;
+    if (gb->n_key_cols == 2) {
+        sl.key1 = off;
+        off += NS * kFastT * ks;
+    }
+    if (vs) {
+        sl.val = off;
+        off += NS * kFastT * vs;
+    }
+    if (ps) {
+        sl.pred = off;
+        off += NS * kFastT * ps;
+    }
+    sl.bytes = stage_bytes;
+
+    const bool has_mm = a.has_min || a.has_max;
+    const size_t slot_bytes = 8 + 4 + (a.has_sum ? 8 : 0) + (has_mm ? (vk_is_32(vk) ? 8 : 16) : 0);
+    const size_t bucket_bytes = 2 * slot_bytes;
+    auto layout_table = [&](AggArgs& x, int NB) {  // offsets of the table arrays; returns the bytes used
+        const size_t S = static_cast<size_t>(NB) * 2;
+        size_t o = 0;
+        x.NB = NB;
+        x.so_keys = static_cast<int32_t>(o); o += S * 8;
+        x.so_mn = static_cast<int32_t>(o); o += has_mm ? S * (vk_is_32(vk) ? 8 : 16) : 0;
+        x.so_cnt = static_cast<int32_t>(o); o += S * 4;
+        x.so_l0 = static_cast<int32_t>(o); o += a.has_sum ? S * 4 : 0;
+        x.so_l1 = static_cast<int32_t>(o); o += a.has_sum ? S * 4 : 0;
+        return (o + 127) & ~size_t(127);
+    };
+
+    // Spill plan: partitions small enough for the spill pass's table (50 KB: four CTAs per SM) at half load.
+    int spill_bits = -1;
+    int NB2 = 0;
+    {
+        const size_t budget2 = static_cast<size_t>(env_int("QDB_SPILL_SMEM_KB", 50)) * 1024 - 1024;  // - the fill prefix
+        NB2 = static_cast<int>(budget2 / bucket_bytes);
+        if (NB2 >= 64 && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
+            const uint64_t per = static_cast<uint64_t>(NB2);  // distinct keys per partition at half load
+            const uint64_t parts = next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per);
+            int bits = 0;
+            while ((1ull << bits) < parts) ++bits;
+            if (bits <= 10) spill_bits = bits;
+        }
+    }
+    const size_t bar_bytes = 128;
+    const size_t list_bytes = static_cast<size_t>(kFastWarps) * kListCap * 2;
+    const size_t spill_words_bytes =
+        spill_bits >= 0 ? ((size_t(4) << spill_bits) + kSeenWords * 4 + 127) & ~size_t(127) : 0;
+    const size_t budget = static_cast<size_t>(di.max_smem_optin) - 1024 - ring - bar_bytes - list_bytes -
+                          spill_words_bytes;
+    int NBmax = static_cast<int>(budget / bucket_bytes);
+    const int64_t forced = env_int("QDB_FAST_BUCKETS", 0);
+    if (forced > 0 && forced < NBmax) NBmax = static_cast<int>(forced);
+    if (NBmax < 64) return QDB_OK;
+    // A table that holds every group at half load or less takes them all (sized for a quarter load when it can);
+    // otherwise the largest table that fits, with the misses spilled by key hash.
+    const uint64_t groups = static_cast<uint64_t>(gb->capacity) + 1;
+    const bool fits = groups <= static_cast<uint64_t>(NBmax);
+    const int NB = fits ? static_cast<int>(std::max<uint64_t>(64, std::min<uint64_t>(NBmax, 2 * groups))) : NBmax;
+    if (fits) spill_bits = -1;
+    const size_t tab_bytes = layout_table(a, NB);
+    a.fits = fits ? 1 : 0;
+    a.probe_b = fits ? 8 : 1;
+    a.dedup = static_cast<int32_t>(env_int("QDB_DEDUP", 2));
+    a.T = kFastT;
+    a.NS = NS;
+    a.sl = sl;
+    a.tiles = (a.n + kFastT - 1) / kFastT;
+    a.full_tiles = a.n / kFastT;
+    a.staged = 1;
+
+    SpillArea* spill = nullptr;
+    if (spill_bits >= 0) {
+        // One cell per (partition, CTA), each holding 5/4 of its share of half this call's rows (at most 2^28 rows in
+        // all) plus 64: warps whose hit rate is below 1/2 stop spilling, and rows of a full cell go to the global table.
+        const int64_t parts = int64_t(1) << spill_bits;
+        const int64_t ctas = std::min<int64_t>(di.sm_count, a.tiles);
+        const int64_t rows = std::min<int64_t>((a.n + 1) / 2, int64_t(1) << 28);
+        const int64_t cell = (rows + rows / 4) / (parts * ctas) + 64;
+        // Records of 16 bytes (key word, value bits), or 8 (the key word) for a count-only table; one more fill word
+        // is the spill pass's work counter.
+        const uint64_t words = static_cast<uint64_t>(parts * ctas * cell) * (vs ? 2 : 1);
+        int32_t rc = spill_acquire(gb->device, words, 0, parts * ctas + 1, s, &spill);
+        if (rc != QDB_OK) return rc;
+        a.spill_keys = spill->keys;
+        a.spill_vals = nullptr;
+        a.spill_fill = spill->fill;
+        a.spill_cell = cell;
+        a.spill_bits = spill_bits;
+        a.spill_ctas = static_cast<int32_t>(ctas);
+    }
+    a.so_bar = static_cast<int32_t>(tab_bytes);
+    a.so_list = static_cast<int32_t>(tab_bytes + bar_bytes);
+    a.so_spill = static_cast<int32_t>(a.so_list + list_bytes);
+    a.so_stage = static_cast<int32_t>(a.so_spill + spill_words_bytes);
+    const size_t smem = a.so_stage + ring;
+    *used = true;
+    int32_t rc = launch_fast(gb, a, ptype, smem, s);
+    if (rc != QDB_OK || spill_bits < 0) {
+        if (spill) spill_release(spill, s);
+        return rc;
+    }
+    // Spill pass: partitions x slices CTAs, each with a table of NB2 buckets.
+    AggArgs b = a;
+    const size_t tab2 = layout_table(b, NB2);
+    b.so_spill = static_cast<int32_t>(tab2);  // the prefix of the cell fills
+    const size_t smem2 = tab2 + ((static_cast<size_t>(a.spill_ctas) + 1) * 4 + 127) / 128 * 128;
+    b.fits = 1;
+    b.probe_b = 8;
+    // Persistent CTAs (four per SM) take (partition, slice) items; a partition is cut into slices only when there are
+    // fewer partitions than CTAs.
+    const int64_t parts = int64_t(1) << spill_bits;
+    const int64_t ctas2 = 4 * static_cast<int64_t>(di.sm_count);
+    const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, ctas2 / parts));
+    rc = launch_fspill(gb, b, smem2, std::min<int64_t>(ctas2, parts * slices), static_cast<int32_t>(slices), s);
+    spill_release(spill, s);
+    return rc;
+}
+
 }  // namespace qdb
 
 using namespace qdb;
@@ -438,6 +607,13 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     a.counters = gb->counters;
     a.capacity = static_cast<unsigned long long>(gb->capacity);
     const bool nulls = a.knull0 || a.knull1 || a.vnull || a.pnull;
+    if (!nulls && !mask && gb->placement != QDB_PLACE_GLOBAL && n >= kFastT && env_int("QDB_AGG_FAST", 1) != 0 &&
+        aligned16(a.key0) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
+        (!a.pcol || aligned16(a.pcol))) {
+        bool used = false;
+        const int32_t rc = process_fast(gb, a, pred, ptype, s, &used);
+        if (rc != QDB_OK || used) return rc;
+    }
 
     // Tile and stage plan: stages of about 32 KB (a stage costs a fixed hand-off between the producer and
     // the consumers, so small stages cannot reach the HBM bandwidth), three of them in the ring.
@@ -512,7 +688,7 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     int spill_bits = -1;
     int S2spill = 0;
     if (smem_place && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
-        const size_t budget2 = static_cast<size_t>(env_int("QDB_SPILL_SMEM_KB", 50)) * 1024;  // 50 KB: four spill-pass CTAs per SM
+        const size_t budget2 = static_cast<size_t>(env_int("QDB_SPILL_SMEM_KB", 50)) * 1024 - 1024;  // - the fill prefix  // 50 KB: four spill-pass CTAs per SM
         int S2 = 1 << 15;
         while (S2 >= 256 && static_cast<size_t>(S2 + 2) * bps + 256 > budget2) S2 >>= 1;
         if (S2 >= 256) {

@@ -94,6 +94,14 @@ struct AggArgs {
     int64_t spill_cell = 0;          // rows per cell
     int32_t spill_bits = 0;          // log2 of the partition count
     int32_t spill_ctas = 0;          // CTAs of the aggregation pass (its grid)
+    // Bucketed table of the fast pass (groupby_fast.cuh): NB buckets of four slots, one 64-bit tag word per
+    // bucket at so_tags, key words at so_keys; counts, sum limbs and min/max at so_cnt, so_l0, so_l1, so_mn.
+    int32_t NB = 0;
+    int32_t so_tags = 0, so_keys = 0;
+    int32_t fits = 0;      // 1: every group fits the table: a key may overflow into the next probe_b - 1 buckets
+    int32_t probe_b = 1;   // buckets a claim may visit
+    int32_t dedup = 2;     // warp aggregation of equal keys: 0 off, 1 on, 2 decided per warp from its first batches
+    int32_t pred_float = 0;  // the fast pass compares IEEE predicate values as order-preserving integers
 };
 
 template <typename A, typename B>
