@@ -116,6 +116,13 @@ int32_t qdb_memcpy_d2h(void* dst, const void* src, int64_t bytes, void* stream);
 int32_t qdb_memcpy_d2d(void* dst, const void* src, int64_t bytes, void* stream);
 int32_t qdb_memset(void* dst, int32_t byte_value, int64_t bytes, void* stream);
 int32_t qdb_stream_sync(void* stream);
+/* Context::bindDeviceToContext / getBoundDeviceID (qikkDB/QueryEngine/Context.cu:134-139): the calling thread's
+ * current device, on which every other entry point works. */
+int32_t qdb_set_device(int32_t device);
+int32_t qdb_get_device(int32_t* out_device);
+/* Synchronous copy between two devices' memory, the transfer the reference's multi-GPU GetResults makes through
+ * host buffers when it gathers every GPU's table (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:594-790). */
+int32_t qdb_memcpy_peer(void* dst, int32_t dst_device, const void* src, int32_t src_device, int64_t bytes);
 
 /* ---- GROUP BY table: GPUGroupBy<AGG,O,K,V> (qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:285-790) and
  *      the multi-key specialisation (qikkDB/QueryEngine/GPUCore/GPUGroupByMultiKey.cuh:262-1325). ----

@@ -118,6 +118,9 @@ SIGNATURES = [
     ("qdb_memcpy_d2d", I32, [P, P, I64, P]),
     ("qdb_memset", I32, [P, I32, I64, P]),
     ("qdb_stream_sync", I32, [P]),
+    ("qdb_set_device", I32, [I32]),
+    ("qdb_get_device", I32, [C.POINTER(I32)]),
+    ("qdb_memcpy_peer", I32, [P, I32, P, I32, I64]),
     ("qdb_gb_create", I32, [PP, I32, I32, I32, I32, I64, I32, P]),
     ("qdb_gb_destroy", I32, [P]),
     ("qdb_gb_max_hash_count", I32, [P, PI64]),

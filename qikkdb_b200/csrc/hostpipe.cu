@@ -80,7 +80,9 @@ extern "C" int32_t qdb_gb_process_host(qdb_gb* gb, const void* const* key_cols, 
     o.total = off;
 
     if (hp->stage_bytes < o.total) {
-        QDB_CUDA_TRY(cudaStreamSynchronize(s));
+        // Earlier calls may have run on other streams: wait for their last use of each buffer and for the copies.
+        for (int b = 0; b < 2; ++b) QDB_CUDA_TRY(cudaEventSynchronize(hp->consumed[b]));
+        QDB_CUDA_TRY(cudaStreamSynchronize(hp->copy));
         for (int b = 0; b < 2; ++b) {
             if (hp->stage[b]) cudaFree(hp->stage[b]);
             hp->stage[b] = nullptr;
@@ -89,8 +91,9 @@ extern "C" int32_t qdb_gb_process_host(qdb_gb* gb, const void* const* key_cols, 
         for (int b = 0; b < 2; ++b) QDB_CUDA_TRY(cudaMalloc(&hp->stage[b], o.total));
         hp->stage_bytes = o.total;
     }
-    // The copy stream must not overwrite a buffer before work already queued on `s` is done with it.
-    for (int b = 0; b < 2; ++b) QDB_CUDA_TRY(cudaEventRecord(hp->consumed[b], s));
+    // consumed[b] keeps the record of the last aggregation that read buffer b, on whichever stream the call that
+    // queued it used, so the copy stream's wait below orders this call after earlier calls on other streams too
+    // (an event never recorded makes the wait a no-op).  It is re-recorded only after this call's own use of b.
 
     const int64_t nchunks = (n + chunk_rows - 1) / chunk_rows;
     for (int64_t c = 0; c < nchunks; ++c) {

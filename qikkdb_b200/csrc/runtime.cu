@@ -139,4 +139,23 @@ int32_t qdb_stream_sync(void* stream) {
     return QDB_OK;
 }
 
+int32_t qdb_set_device(int32_t device) {
+    QDB_CUDA_TRY(cudaSetDevice(device));
+    return QDB_OK;
+}
+
+int32_t qdb_get_device(int32_t* out_device) {
+    if (!out_device) return fail(QDB_ERR_INVALID, "qdb_get_device: null out_device");
+    int d = 0;
+    QDB_CUDA_TRY(cudaGetDevice(&d));
+    *out_device = d;
+    return QDB_OK;
+}
+
+int32_t qdb_memcpy_peer(void* dst, int32_t dst_device, const void* src, int32_t src_device, int64_t bytes) {
+    if (bytes <= 0) return QDB_OK;
+    QDB_CUDA_TRY(cudaMemcpyPeer(dst, dst_device, src, src_device, static_cast<size_t>(bytes)));
+    return QDB_OK;
+}
+
 }  // extern "C"

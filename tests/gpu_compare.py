@@ -42,7 +42,6 @@ def compare(gpu: dict, ref: dict, aggs, val_is_float: bool, key_is_float: bool =
         if val_is_float and a in ("sum", "avg"):
             denom = np.maximum(np.abs(r[ok]), 1e-30)
             rel = np.abs(g[ok].astype(np.float64) - r[ok]) / denom
-            # sums whose true value is ~0 through cancellation are judged on the absolute scale
             if rel.size:
                 max_rel = max(max_rel, float(rel.max()))
             assert (rel <= rtol).all(), f"{a}: max relative error {rel.max():.3e} > {rtol}"

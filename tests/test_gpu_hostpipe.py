@@ -41,3 +41,24 @@ def test_host_columns_pinned_with_nulls(cuda):
     t.check()
     r = oracle.groupby(k.numpy(), v.numpy(), key_nulls=[kw], val_nulls=vw)
     compare(t.results_numpy(), r, ALL, False)
+
+
+def test_host_columns_back_to_back_on_two_streams(cuda):
+    # The staging buffers are shared by every call of a thread: a call on a second stream must not overwrite a
+    # buffer that the first stream's aggregation still reads.
+    n = (1 << 21) + 4099
+    k1 = dg.zipf_i64(103, 0, n, 400_000, 1.1)
+    v1 = dg.lognormal_f32(103, 1, n, 2.0, 1.0)
+    k2 = dg.zipf_i64(104, 0, n, 50_000, 1.3)
+    v2 = dg.lognormal_f32(104, 1, n, 1.0, 2.0)
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    ta = GroupByTable(ALL, np.int64, np.float32, 1 << 19)
+    tb = GroupByTable(ALL, np.int64, np.float32, 1 << 16)
+    torch.cuda.synchronize()
+    ta.process_host([k1], v1, chunk_rows=1 << 18, stream=sa.cuda_stream)
+    tb.process_host([k2], v2, chunk_rows=1 << 18, stream=sb.cuda_stream)
+    torch.cuda.synchronize()
+    ta.check()
+    tb.check()
+    assert compare(ta.results_numpy(), oracle.groupby(k1, v1), ALL, True) <= FLOAT_RTOL
+    assert compare(tb.results_numpy(), oracle.groupby(k2, v2), ALL, True) <= FLOAT_RTOL

@@ -2,8 +2,9 @@
 
 qdb_reconstruct_keep_noalloc serves callers that own all device memory themselves (a buffer pool that accounts
 every byte, a serving loop with a fixed HBM budget) and therefore cannot let the library allocate during a query.
-It must select exactly what qdb_reconstruct_keep selects.  Two calls run back to back, because every call shares
-one scratch array that keeps the previous call's contents.  This file is collected last on purpose.
+It must select exactly what qdb_reconstruct_keep selects and what the CPU oracle's compaction selects.  Two calls
+run back to back, because every call shares one scratch array that keeps the previous call's contents.  This file
+is collected last on purpose.
 """
 import ctypes as C
 
@@ -11,6 +12,7 @@ import numpy as np
 import pytest
 import torch
 
+import oracle
 from qikkdb_b200 import _capi
 from qikkdb_b200.groupby import nullmask_words, pack_nullmask, unpack_nullmask
 
@@ -68,3 +70,34 @@ def test_noalloc_rejects_oversize_and_short_output(cuda):
     rc = lib.qdb_reconstruct_keep_noalloc(4, col.data_ptr(), mask.data_ptr(), 1000, out.data_ptr(), 10,
                                           C.byref(cnt), None, None, stream)
     assert rc == _capi.QDB_ERR_TOO_LARGE
+
+
+def test_noalloc_compaction_matches_oracle_unaligned_mask(cuda):
+    # A mask that starts one byte past a 16-byte boundary takes the kernels' scalar path, and row counts that are not
+    # a multiple of the 4096-row tile leave a ragged last tile.
+    lib = _capi.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(78)
+    for call, (n, dtype, density) in enumerate([(700_001, np.int32, 0.5), (12_345, np.float64, 0.07)]):
+        col_h = (rng.standard_normal(n) * 1e4).astype(dtype)
+        mask_h = (rng.random(n) < density).astype(np.int8)
+        nulls_flags = rng.random(n) < 0.1
+        words_h = pack_nullmask(nulls_flags)
+        exp_vals, exp_words, exp_n = oracle.compact(col_h, mask_h, words_h)
+        col = torch.from_numpy(col_h).cuda()
+        mask_buf = torch.zeros(n + 16, dtype=torch.int8, device="cuda")
+        mask_buf[1:n + 1] = torch.from_numpy(mask_h).cuda()
+        mask = mask_buf[1:n + 1]
+        assert mask.data_ptr() % 16 == 1
+        nulls = torch.from_numpy(words_h.view(np.int64)).cuda()
+        out = torch.full((n,), 3, dtype=col.dtype, device="cuda")
+        out_nulls = torch.full((nullmask_words(n),), -1, dtype=torch.int64, device="cuda")
+        cnt = C.c_int64(-1)
+        _capi.check(lib.qdb_reconstruct_keep_noalloc(col.element_size(), col.data_ptr(), mask.data_ptr(), n,
+                                                     out.data_ptr(), n, C.byref(cnt), nulls.data_ptr(),
+                                                     out_nulls.data_ptr(), stream))
+        torch.cuda.synchronize()
+        assert cnt.value == exp_n, f"call {call}: count {cnt.value} != {exp_n}"
+        assert (out[:exp_n].cpu().numpy() == exp_vals).all(), f"call {call}: compacted values differ from the oracle"
+        got_nulls = unpack_nullmask(out_nulls.cpu().numpy(), exp_n)
+        assert (got_nulls == unpack_nullmask(exp_words, exp_n)).all(), f"call {call}: null bits differ from the oracle"
