@@ -1,19 +1,25 @@
 #!/usr/bin/env python
 """Filtered GROUP BY benchmark (one JSON line on rank 0).
 
-Workload (the filtered GROUP BY at scale): 256M rows per GPU; float32 predicate column uniform in [0, 1) with
-WHERE p < 0.5; int64 keys Zipf(s = 1.1) over 1M distinct values; float32 lognormal(mu = 2, sigma = 1) values;
-SUM and AVG (FP64 accumulation) in one global hash table.  Inputs are seeded synthetic columns generated on
-the host; 16 bytes per row (4.3 GB per GPU), larger than L2, so no flush is needed between steps.
+Headline workload (the filtered GROUP BY at scale): 256M rows per GPU; float32 predicate column uniform in [0, 1)
+with WHERE p < 0.5; int64 keys Zipf(s = 1.1) over 1M distinct values; float32 lognormal(mu = 2, sigma = 1) values;
+SUM and AVG (FP64 accumulation) in one global hash table.  Inputs are seeded synthetic columns generated on the
+host; 16 bytes per row (4.3 GB per GPU), larger than L2, so no flush is needed between steps.
 
 A step = one whole query on device-resident columns: table reset, the fused filter + aggregation pass, and
 GetResults (result compaction, count read back).  With --gpus N (torchrun, one rank per GPU) every rank
 aggregates its own 256M-row shard, then the partial tables are exchanged by key owner with NCCL all-to-all and
 merged (weak scaling).  `e2e` measures the same query through the C ABI from pinned HOST columns
 (qdb_gb_process_host: chunked H2D overlapped with aggregation) including the D2H of the result columns.
+`cpu_baseline` runs the oracle over every row of the workload and its result checks the GPU's (`parity`).
+
+On one GPU the same line also carries the other configurations, each measured after the headline:
+`plain_1m` (2^20 rows, int32 keys over 1000 values, cold and warm), `composite_128m` (2^27 rows, 4096 x 4096
+composite keys), `batched` (4096 instances in one CUDA graph against the plain path looped in C) and `served`
+(continuous batching over 2^30 resident rows at four Poisson rates); --headline-only skips them.
 
 --impl reference times the reference's CPU-side GROUP BY (the hash-map aggregation its tests check against,
-restated in oracle/) on all host threads over a bounded sample of the same workload.
+restated in oracle/) on all host threads over the same workload.
 """
 from __future__ import annotations
 
@@ -35,6 +41,7 @@ import numpy as np  # noqa: E402
 ROWS = 1 << 28
 N_DISTINCT = 1_000_000
 BYTES_PER_ROW = 16  # 4 (predicate) + 8 (key) + 4 (value)
+FLOAT_RTOL = 1e-5  # float SUM/AVG against the FP64 oracle
 SEED = 20240601
 METRIC = "filtered GROUP BY rows/s"
 BATCH_INSTANCES = 4096
@@ -53,7 +60,10 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=ROWS)
-    ap.add_argument("--cpu-sample-rows", type=int, default=1 << 25)
+    ap.add_argument("--cpu-sample-rows", type=int, default=0,
+                    help="rows of the CPU baseline (0 = every row; then its result also checks the GPU's)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the plain, composite, batched and served sub-workloads of the default run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served"])
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
@@ -166,31 +176,63 @@ def profiled_traffic():
         return None
 
 
-def cpu_baseline(cols, sample_rows: int) -> dict:
+def cpu_baseline_and_parity(cols, table, sample_rows: int):
+    """The cpu_baseline leg: the oracle (the hash-map GROUP BY the reference's tests check against, all host threads)
+    over the first sample_rows rows of the workload (every row by default), timed.  When it covered every row its
+    result is also the checker of this run's GPU result: keys and COUNT exactly, SUM and AVG as the largest relative
+    error over the groups (the per-query error), against the 1e-5 bound."""
     import oracle
-    n = min(sample_rows, cols["key"].numel())
+    n = min(sample_rows, cols["key"].numel()) if sample_rows > 0 else cols["key"].numel()
     p = cols["pred"].numpy()[:n]
     k = cols["key"].numpy()[:n]
     v = cols["val"].numpy()[:n]
-    r = oracle.groupby(k, v, pred=(p, 2, 0.5, np.float32, None), threads=0, sort=False, timing_only=True)
-    return {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
-            "sample": f"first {n} rows of the workload (same columns), hash-map GROUP BY, {r['threads']} threads, "
-                      f"{r['seconds']:.3f} s"}
+    full = n == cols["key"].numel()
+    r = oracle.groupby(k, v, pred=(p, 2, 0.5, np.float32, None), threads=0, sort=full, timing_only=not full)
+    cpu = {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+           "sample": f"{'all' if full else 'first'} {n} rows of the workload (same columns), hash-map GROUP BY, "
+                     f"{r['threads']} threads, {r['seconds']:.3f} s"}
+    if not full:
+        return cpu, None
+    g = table.results_numpy(["sum", "avg", "count"])
+    order = np.argsort(g["keys"][0], kind="stable")
+    same_groups = g["n_groups"] == r["count"]
+    keys_equal = bool(same_groups and (g["keys"][0][order] == r["keys"][0]).all())
+    count_equal = bool(keys_equal and (g["count"][order] == r["cnt"]).all())
+    rel = {}
+    if keys_equal:
+        for a in ("sum", "avg"):
+            rel[a] = float((np.abs(g[a][order] - r[a]) / np.abs(r[a])).max())
+    ok = keys_equal and count_equal and max(rel.values(), default=1.0) <= FLOAT_RTOL
+    parity = {"checked_against": "oracle (FP64 hash-map GROUP BY) over every row", "groups": int(g["n_groups"]),
+              "keys_equal": keys_equal, "count_equal": count_equal, "max_rel_err": rel, "rtol": FLOAT_RTOL,
+              "parity": bool(ok)}
+    return cpu, parity
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU-side GROUP BY (the hash-map aggregation its tests check against,
+    restated in oracle/) on all host threads over the same 256M-row workload.  A step aggregates every row; only if
+    K + W such steps would take more than four minutes does a step take a leading sample of the rows instead."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     import oracle
-    n = args.cpu_sample_rows
-    cols = gen_columns(n, 0, pinned=False)
+    n_all = args.rows
+    cols = gen_columns(n_all, 0, pinned=False)
     p, k, v = cols["pred"].numpy(), cols["key"].numpy(), cols["val"].numpy()
+
+    def one(n):
+        return oracle.groupby(k[:n], v[:n], pred=(p[:n], 2, 0.5, np.float32, None), threads=0, sort=False,
+                              timing_only=True)
+
+    first = one(n_all)
+    n = n_all
+    if (args.warmup + args.steps) * first["seconds"] > 240.0:
+        n = max(1 << 20, int(n_all * 240.0 / ((args.warmup + args.steps) * first["seconds"])))
     secs = []
-    threads = 0
+    threads = first["threads"]
     for i in range(args.warmup + args.steps):
-        r = oracle.groupby(k, v, pred=(p, 2, 0.5, np.float32, None), threads=0, sort=False, timing_only=True)
-        threads = r["threads"]
+        r = first if (i == 0 and n == n_all) else one(n)
         if i >= args.warmup:
             secs.append(r["seconds"])
     t = statistics.mean(secs)
@@ -198,9 +240,11 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rows_per_step": n, "sample_of_rows": args.rows},
+            "config": {"workload": WORKLOAD, "rows_per_step": n, "rows_of_workload": n_all,
+                       "same_config": n == n_all},
             "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                             "sample": f"{n} rows of the workload per step, all host threads"},
+                             "sample": f"{'all' if n == n_all else 'first'} {n} rows of the workload per step, "
+                                       f"all host threads"},
             "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -270,6 +314,7 @@ def run_ours(args):
         end.record(stream)
         torch.cuda.synchronize()
     launches = lib.qdb_launch_count() - launches0
+    clocks = sampler.summary()
     ms = start.elapsed_time(end) / args.steps
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -319,10 +364,24 @@ def run_ours(args):
     achieved = n * BYTES_PER_ROW / t_agg / 1e9
     traffic = profiled_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "gb_agg_kernel + gb_spill_kernel (fused filter + shared-table aggregate, spill merge)",
+                "traffic": traffic, "kernel": "gb_fast_kernel + gb_fspill_kernel (fused filter + shared-table aggregate, spill pass)",
                 "kernel_ms": t_agg * 1e3, "algorithmic_bytes_per_launch": n * BYTES_PER_ROW,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, copy bandwidth)"}
-    cpu = cpu_baseline(cols, args.cpu_sample_rows) if (rank == 0 and world == 1) else None
+    cpu, parity = (cpu_baseline_and_parity(cols, table, args.cpu_sample_rows) if (rank == 0 and world == 1)
+                   else (None, None))
+    subs = {}
+    if world == 1 and not args.headline_only:
+        # The other configurations of the workload family, each measured on its own after the headline's columns
+        # are released: plain 1M-row GROUP BY (cold and warm), the 128M-row composite key, batched and served.
+        del dcols, table, pred
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        subs["plain_1m"] = c0_measure(args, dev)
+        subs["composite_128m"] = c2_measure(args, dev)
+        torch.cuda.empty_cache()
+        subs["batched"] = batched_measure(args, dev, sub=True)
+        torch.cuda.empty_cache()
+        subs["served"] = served_measure(args, dev, sub=True)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -330,12 +389,139 @@ def run_ours(args):
                 "config": {"workload": WORKLOAD, "rows_per_gpu": n, "global_rows": world * n, "groups": int(groups),
                            "parallelism": f"dp{world}" if world > 1 else "single", "l2": "inputs (4.3 GB) > L2, no flush",
                            "step": "reset + fused filter/aggregate + exchange (N>1) + GetResults"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": sampler.summary(),
-                "gpu_launches": int(launches)}
+                "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": int(launches), **subs}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# The plain 1M-row GROUP BY (cold and warm) and the 128M-row composite-key GROUP BY, measured after the headline.
+# ---------------------------------------------------------------------------------------------------------------
+C0_SEED = 20240604
+C0_WORKLOAD = ("plain-groupby-1M: 2^20 rows, int32 key uniform in [0,1000), int32 value uniform in [-1000,1000]; "
+               "SUM+MIN+MAX+COUNT in one table, one block")
+C2_SEED = 20240605
+C2_WORKLOAD = ("composite-groupby-128M: 2^27 rows, (int32 uniform in [0,4096), int32 uniform in [0,4096)) keys "
+               "(~16.8M groups), int64 value uniform in [0,2^31); SUM+COUNT+MAX")
+
+
+def _event_steps(fn, steps: int, warmup: int, before=None):
+    """Device time (ms) of each of `steps` calls of fn after `warmup` untimed ones; `before` runs outside the timed
+    region ahead of every call (an L2 flush)."""
+    import torch
+    for _ in range(warmup):
+        if before:
+            before()
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(steps):
+        if before:
+            before()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def _exact_parity(g: dict, r: dict, aggs) -> dict:
+    """Integer GROUP BY results against the oracle's: group count, keys and every aggregate bit for bit."""
+    ok = g["n_groups"] == r["count"]
+    if ok:
+        order = np.lexsort([np.asarray(k, np.int64) for k in reversed(g["keys"])])
+        ok = all((np.asarray(gk, np.int64)[order] == rk).all() for gk, rk in zip(g["keys"], r["keys"]))
+        for a in aggs:
+            ok = ok and bool((np.asarray(g[a], np.int64)[order] == r["cnt" if a == "count" else a]).all())
+    return {"checked_against": "oracle (hash-map GROUP BY) over every row", "groups": int(g["n_groups"]),
+            "exact": bool(ok), "parity": bool(ok)}
+
+
+def c0_measure(args, dev) -> dict:
+    import torch
+
+    import oracle
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import GroupByTable
+    n = 1 << 20
+    aggs = ["sum", "min", "max", "count"]
+    k = dg.uniform_i32(C0_SEED, 0, n, 0, 999)
+    v = dg.uniform_i32(C0_SEED, 1, n, -1000, 1000)
+    dk, dv = torch.from_numpy(k).to(dev), torch.from_numpy(v).to(dev)
+    t = GroupByTable(aggs, np.int32, np.int32, 1000)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # twice the L2
+
+    def step():
+        t.reset()
+        t.process([dk], dv, n, sync=False)
+        t.results(aggs)
+
+    warm = _event_steps(step, args.steps, args.warmup)
+    cold = _event_steps(step, args.steps, args.warmup, before=lambda: flush.fill_(1))
+    g = t.results_numpy(aggs)
+    # cpu_baseline leg: the oracle over the same 1M rows, timed; its result checks the GPU result bit for bit
+    r = oracle.groupby(k, v, threads=0)
+    wm, cm = statistics.median(warm), statistics.median(cold)
+    return {"workload": C0_WORKLOAD, "metric": "plain GROUP BY rows/s", "unit": "rows/s",
+            "warm": {"value": n / (wm / 1e3), "ms_per_step": wm},
+            "cold": {"value": n / (cm / 1e3), "ms_per_step": cm, "l2": "256 MB written before every step"},
+            "step": "reset + fused aggregate + GetResults (4 aggregates, one pass)",
+            "bytes_per_row": 8,
+            "cpu_baseline": {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                             "sample": f"all {n} rows, hash-map GROUP BY, {r['threads']} threads"},
+            "parity": _exact_parity(g, r, aggs)}
+
+
+def c2_measure(args, dev) -> dict:
+    import torch
+
+    import oracle
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import GroupByTable
+    n = 1 << 27
+    aggs = ["sum", "count", "max"]
+    a = dg.uniform_i32(C2_SEED, 0, n, 0, 4095)
+    b = dg.uniform_i32(C2_SEED, 1, n, 0, 4095)
+    v = dg.uniform_i64(C2_SEED, 2, n, 0, (1 << 31) - 1)
+    da, db, dv = (torch.from_numpy(x).to(dev) for x in (a, b, v))
+    t = GroupByTable(aggs, np.int32, np.int64, 1 << 24, n_key_cols=2)
+    agg_ms = []
+
+    def step():
+        t.reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        t.process([da, db], dv, n, sync=False)
+        e1.record()
+        t.results(aggs)
+        agg_ms.append((e0, e1))
+
+    ms = _event_steps(step, args.steps, args.warmup)
+    kms = statistics.median(x.elapsed_time(z) for x, z in agg_ms[args.warmup:])
+    t.check()
+    g = t.results_numpy(aggs)
+    del da, db, dv
+    peak, peak_kind = measured_peak()
+    out = {"workload": C2_WORKLOAD, "metric": "composite GROUP BY rows/s", "unit": "rows/s",
+           "value": n / (statistics.median(ms) / 1e3), "ms_per_step": statistics.median(ms),
+           "step": "reset + aggregation (partition pass + spill pass) + GetResults", "groups": int(g["n_groups"]),
+           "roofline": {"bound": "hbm", "achieved": n * 16 / (kms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": n * 16 / (kms / 1e3) / 1e9 / peak, "kernel_ms": kms,
+                        "algorithmic_bytes_per_launch": n * 16, "peak_kind": peak_kind},
+           "global_updates_per_s": n / (kms / 1e3)}
+    # cpu_baseline leg: the oracle over every row, timed; its result checks the GPU result bit for bit
+    r = oracle.groupby([a, b], v, threads=0)
+    out["cpu_baseline"] = {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                           "sample": f"all {n} rows, hash-map GROUP BY, {r['threads']} threads, {r['seconds']:.1f} s"}
+    out["parity"] = _exact_parity(g, r, aggs)
+    return out
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -400,19 +586,24 @@ def batched_columns(shapes, dev, host: bool = False):
 
 
 def run_batched(args):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    line = batched_measure(args, torch.device("cuda", local))
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps(line), flush=True)
+
+
+def batched_measure(args, dev, sub: bool = False) -> dict:
+    """The batched workload on `dev`: every instance in one CUDA graph (value: queries/s, device-timed), end to end
+    with the results copied to host, against the same queries one by one through the plain path looped in C."""
     import ctypes as C
 
     import torch
 
     from qikkdb_b200 import _capi
-    from qikkdb_b200.batch import GroupByBatch, Query, required_bytes
-    from qikkdb_b200.groupby import AGG_CODES
+    from qikkdb_b200.batch import GroupByBatch, Query, plain_run, required_bytes
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     lib = _capi.lib()
     shapes = batched_instances(args.instances)
     views, _, bufs = batched_columns(shapes, dev)
@@ -434,7 +625,7 @@ def run_batched(args):
     counts, status = b.fetch(stream=st.cuda_stream)
     assert (status == 0).all(), "batched run reported an error status"
     launches0 = lib.qdb_launch_count()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(dev.index or 0)
     ev = []
     with sampler:
         for _ in range(args.steps):
@@ -446,7 +637,7 @@ def run_batched(args):
             ev.append((e0, e1))
         torch.cuda.synchronize(dev)
     launches = lib.qdb_launch_count() - launches0
-    step_ms = [a.elapsed_time(z) for a, z in ev]
+    step_ms = [x.elapsed_time(z) for x, z in ev]
     ms = statistics.median(step_ms)
     value = len(queries) / (ms / 1e3)
     groups = int(counts.sum())
@@ -466,62 +657,34 @@ def run_batched(args):
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
     em = statistics.median(e2e_ms)
 
-    # the same queries one by one through the plain path (create, ProcessBlock + Swap, GetResults, free)
-    sample = list(range(len(queries))) if args.plain_sample <= 0 else list(range(min(args.plain_sample, len(queries))))
-    outs = (C.c_void_p * 8)()
-    onulls = (C.c_void_p * 8)()
-    okeys = (C.c_void_p * 1)()
-    oknull = (C.c_void_p * 1)()
-    cnt = C.c_int64()
-    plain_groups = 0
-
-    def plain_pass():
-        nonlocal plain_groups
-        plain_groups = 0
-        for i in sample:
-            r, c, vdt, aggs = shapes[i]
-            kd, vd = views[i]
-            mask = 0
-            for a in aggs:
-                mask |= AGG_CODES[a]
-            h = C.c_void_p()
-            vt = _capi.QDB_INT64 if vdt == np.int64 else _capi.QDB_FLOAT
-            _capi.check(lib.qdb_gb_create(C.byref(h), mask, _capi.QDB_INT32, 1, vt, c, 0, st.cuda_stream))
-            kc = (C.c_void_p * 1)(kd.data_ptr())
-            _capi.check(lib.qdb_gb_process_sync(h, kc, None, vd.data_ptr(), None, r, None, None, st.cuda_stream))
-            codes = (C.c_int32 * len(aggs))(*[AGG_CODES[a] for a in aggs])
-            _capi.check(lib.qdb_gb_results_multi(h, len(aggs), codes, okeys, oknull, outs, onulls, C.byref(cnt),
-                                                 st.cuda_stream))
-            plain_groups += cnt.value
-            lib.qdb_free(okeys[0], st.cuda_stream)
-            for j in range(len(aggs)):
-                lib.qdb_free(outs[j], st.cuda_stream)
-            lib.qdb_gb_destroy(h)
-        torch.cuda.synchronize(dev)
-
-    plain_pass()  # warm-up (pool allocations, module load)
+    # the same queries one by one through the plain path, the loop in C (no per-query Python): results to host
+    sample = queries if args.plain_sample <= 0 else queries[:args.plain_sample]
+    plain_run(sample[:8], stream=st.cuda_stream)  # warm-up (pool allocations, module load)
     t0 = time.perf_counter()
-    plain_pass()
+    pg = plain_run(sample, results_to_host=True, stream=st.cuda_stream)
     plain_s = time.perf_counter() - t0
     plain_qps = len(sample) / plain_s
-    if not args.plain_sample:
-        assert plain_groups == groups, f"plain path groups {plain_groups} != batched {groups}"
+    if len(sample) == len(queries):
+        assert int(pg.sum()) == groups, f"plain path groups {int(pg.sum())} != batched {groups}"
 
     peak, peak_kind = measured_peak()
     achieved = bytes_total / (ms / 1e3) / 1e9
-    cpu = batched_cpu_baseline(shapes, args) if rank == 0 and world == 1 else None
+    cpu = batched_cpu_baseline(shapes, args, budget_s=5.0 if sub else 15.0)
+    del b, views, bufs
     line = {"metric": BATCH_METRIC, "value": value, "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "replicas only",
             "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
             "config": {"workload": BATCH_WORKLOAD, "instances": len(queries), "rows_total": rows_total,
-                       "bytes_total": bytes_total, "groups_total": groups, "l2": f"inputs ({bytes_total / 1e9:.1f} GB) > L2, no flush",
+                       "bytes_total": bytes_total, "groups_total": groups,
+                       "l2": f"inputs ({bytes_total / 1e9:.1f} GB) > L2, no flush",
                        "step": "one CUDA graph: table init (skipped after the first run) + persistent aggregation "
                                "kernel + result kernel, all instances"},
             "plain_one_by_one": {"value": plain_qps, "unit": "queries/s", "queries": len(sample),
-                                 "seconds": plain_s, "groups": plain_groups,
-                                 "path": "per query: qdb_gb_create, qdb_gb_process_sync, qdb_gb_results_multi, "
-                                         "qdb_free, qdb_gb_destroy (ctypes, wall clock)"},
+                                 "seconds": plain_s, "groups": int(pg.sum()),
+                                 "path": "qdb_gb_plain_run: per query qdb_gb_create, qdb_gb_process_sync, "
+                                         "qdb_gb_results_multi, results to host, qdb_free, qdb_gb_destroy (loop in C)"},
             "speedup_vs_plain": value / plain_qps,
+            "e2e_speedup_vs_plain": (len(queries) / (em / 1e3)) / plain_qps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "whole graph (init + gb_batch_agg_kernel + results)",
                          "algorithmic_bytes_per_launch": bytes_total, "peak_kind": peak_kind},
@@ -532,8 +695,7 @@ def run_batched(args):
                             "inputs device-resident"},
             "set_ms": set_ms, "autotune_s": tune_s, "clocks": sampler.summary(), "gpu_launches": int(launches),
             "step_ms_min_max": [min(step_ms), max(step_ms)]}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def batched_cpu_baseline(shapes, args, budget_s: float = 15.0) -> dict:
@@ -630,17 +792,24 @@ def served_queries(cols, n_q: int, seed: int):
 
 
 def run_served(args):
-    import ctypes as C
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    print(json.dumps(served_measure(args, torch.device("cuda", local))), flush=True)
+
+
+def served_measure(args, dev, sub: bool = False) -> dict:
+    """The served workload on `dev`: closed-burst capacity and four open-loop Poisson rates through the serving loop
+    (latencies from arrival to results on the host), against the same kind of queries one by one through the plain
+    path looped in C (results to host)."""
+    import dataclasses
 
     import torch
 
     from qikkdb_b200 import _capi
-    from qikkdb_b200.groupby import AGG_CODES
+    from qikkdb_b200.batch import plain_run
     from qikkdb_b200.serve import Server, percentile_ms, poisson_arrivals
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     lib = _capi.lib()
     n = args.served_rows
     cols = served_columns(n, dev)
@@ -651,12 +820,13 @@ def run_served(args):
     srv.run_open_loop(warm, np.zeros(len(warm), np.int64))
     burst = served_queries(cols, n_q, SERVE_SEED + 1)
     launches0 = lib.qdb_launch_count()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(dev.index or 0)
     with sampler:
         lat, stat, wall = srv.run_open_loop(burst, np.zeros(n_q, np.int64))
     launches = lib.qdb_launch_count() - launches0
     assert (stat == 0).all(), f"served queries failed: {np.unique(stat)}"
     capacity = n_q / (wall / 1e9)
+    burst_p50, burst_p99 = percentile_ms(lat, 50), percentile_ms(lat, 99)
     rates = []
     for k, frac in enumerate((0.25, 0.5, 0.75, 0.95)):
         rate = capacity * frac
@@ -668,56 +838,16 @@ def run_served(args):
     st = srv.stats()
     srv.close()
 
-    # the same kind of queries one by one through the plain path: key % c column (GPUBinary mod), table created
-    # with the query's true group bound, ProcessBlock with the fused WHERE, GetResults, results to host, free
-    plain = served_queries(cols, args.plain_sample or 24, SERVE_SEED + 1)
-    tmp = {"k32": torch.empty(n, dtype=torch.int32, device=dev), "k64": torch.empty(n, dtype=torch.int64, device=dev)}
+    # the same queries one by one through the plain path (loop in C): key % c column, a table with the query's true
+    # group bound, ProcessBlock with the fused WHERE, GetResults, results to host, everything freed
+    plain = [dataclasses.replace(q, max_groups=min(q.key_mod, n)) for q in burst[:args.plain_sample or 32]]
     s0 = torch.cuda.current_stream().cuda_stream
-    outs = (C.c_void_p * 8)()
-    onulls = (C.c_void_p * 8)()
-    okeys = (C.c_void_p * 1)()
-    oknull = (C.c_void_p * 1)()
-    cnt = C.c_int64()
-    from qikkdb_b200.groupby import make_pred
-
-    def plain_pass():
-        for q in plain:
-            kc = "k32" if q.keys.dtype == torch.int32 else "k64"
-            kt = _capi.QDB_INT32 if kc == "k32" else _capi.QDB_INT64
-            _capi.check(lib.qdb_arith_mod(kt, q.keys.data_ptr(), q.key_mod, tmp[kc].data_ptr(), n, s0))
-            mask = 0
-            for a in q.aggs:
-                mask |= AGG_CODES[a]
-            h = C.c_void_p()
-            _capi.check(lib.qdb_gb_create(C.byref(h), mask, kt, 1, _capi.QDB_FLOAT, min(q.key_mod, n), 0, s0))
-            p = make_pred(q.pred[0], q.pred[1], q.pred[2], q.pred[3])
-            kcol = (C.c_void_p * 1)(tmp[kc].data_ptr())
-            _capi.check(lib.qdb_gb_process_sync(h, kcol, None, q.vals.data_ptr(), None, n, C.byref(p), None, s0))
-            codes = (C.c_int32 * len(q.aggs))(*[AGG_CODES[a] for a in q.aggs])
-            _capi.check(lib.qdb_gb_results_multi(h, len(q.aggs), codes, okeys, oknull, outs, onulls, C.byref(cnt), s0))
-            g = cnt.value
-            host = np.empty(max(g, 1) * (1 + len(q.aggs)), np.int64)
-            if g:
-                _capi.check(lib.qdb_memcpy_d2h(host.ctypes.data, okeys[0], g * (4 if kc == "k32" else 8), s0))
-                for j, a in enumerate(q.aggs):  # COUNT is int64, the other aggregates of f32 values are float
-                    _capi.check(lib.qdb_memcpy_d2h(host.ctypes.data + 8 * g * (j + 1), outs[j],
-                                                   g * (8 if a == "count" else 4), s0))
-            lib.qdb_free(okeys[0], s0)
-            for j in range(len(q.aggs)):
-                lib.qdb_free(outs[j], s0)
-            lib.qdb_gb_destroy(h)
-        torch.cuda.synchronize(dev)
-
-    plain_pass_first = plain[:2]
-    saved = plain
-    plain = plain_pass_first
-    plain_pass()
-    plain = saved
+    plain_run(plain[:2], stream=s0)
     t0 = time.perf_counter()
-    plain_pass()
+    plain_run(plain, results_to_host=True, stream=s0)
     plain_s = time.perf_counter() - t0
     plain_qps = len(plain) / plain_s
-    peak, peak_kind = measured_peak()
+    del cols
     line = {"metric": SERVE_METRIC, "value": capacity, "unit": "queries/s", "n_gpus": 1, "steps": 1,
             "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "replicas only",
             "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
@@ -725,15 +855,17 @@ def run_served(args):
                        "in_flight_batches": 2, "table_budget_bytes": 40 << 30,
                        "tables": "sized by the server's cardinality estimate (sampled GEE, capped by the modulus)"},
             "value_is": "closed-burst capacity: all queries submitted at t=0, queries / (first arrival to last result)",
+            "burst_p50_ms": burst_p50, "burst_p99_ms": burst_p99,
             "rates": rates,
             "plain_one_by_one": {"value": plain_qps, "unit": "queries/s", "queries": len(plain), "seconds": plain_s,
-                                 "path": "per query: qdb_arith_mod (key % c column), qdb_gb_create (true bound), "
-                                         "qdb_gb_process_sync (fused WHERE), qdb_gb_results_multi, D2H, qdb_free"},
+                                 "path": "qdb_gb_plain_run: per query qdb_arith_mod (key % c column), qdb_gb_create "
+                                         "(true bound), qdb_gb_process_sync (fused WHERE), qdb_gb_results_multi, "
+                                         "results to host, qdb_free (loop in C)"},
             "speedup_vs_plain": capacity / plain_qps, "server_stats": st,
             "e2e": {"value": capacity, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
                     "path": "qdb_server_run_open_loop: results on the host per query; columns device-resident"},
             "clocks": sampler.summary(), "gpu_launches": int(launches)}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_served_reference(args):

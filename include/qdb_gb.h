@@ -330,6 +330,14 @@ int32_t qdb_gb_batch_required(const qdb_gb_query* queries, int32_t n, int64_t* t
 int32_t qdb_gb_batch_set_sharing(qdb_gb_batch* b, int32_t share);
 /* Clears the process-wide tuning table (plans fall back to the built-in heuristic). */
 int32_t qdb_gb_batch_tuning_reset(void);
+/* The one-query-at-a-time path the batch replaces, looped in C: for each query in turn, as the dispatcher runs a
+ * GROUP BY (GpuSqlDispatcherAggregationFunctions.h:377-507): the `key % key_mod` column when key_mod > 0
+ * (GPUBinary<mod>), a table of max_groups (qdb_gb_create), ProcessBlock with the fused WHERE and the Swap check
+ * (qdb_gb_process_sync), GetResults of every aggregate (qdb_gb_results_multi), with results_to_host != 0 the keys
+ * and aggregate columns copied to host memory, then every buffer freed and the table destroyed.  out_groups[i]
+ * (optional) receives query i's group count.  Returns at the first failing query; synchronises `stream`. */
+int32_t qdb_gb_plain_run(const qdb_gb_query* queries, int32_t n, int32_t results_to_host, int64_t* out_groups,
+                         void* stream);
 
 /* ---- serving loop: continuous batching of GROUP BY queries over device-resident columns ----
  * No counterpart in the reference: its server hands every query to a dispatcher that runs the operators one
@@ -362,8 +370,12 @@ typedef struct qdb_server_result {
 typedef struct qdb_server_stats {
     int64_t submitted, completed, batches, retries, rejected;
     int64_t queries_in_batches; /* sum of batch sizes (mean batch size = queries_in_batches / batches) */
+    int64_t table_budget_bytes; /* the table budget the server admits against (after the free-HBM cut) */
+    int64_t hbm_free_at_create; /* free device memory when the server was created (cudaMemGetInfo) */
 } qdb_server_stats;
 
+/* table_budget_bytes is cut down to the device memory free at creation less a reserve (an eighth of the free
+ * memory, at least 2 GiB) and the result budget; <= 0 takes all of that.  QDB_ERR_NOMEM when nothing is left. */
 int32_t qdb_server_create(qdb_server** out, int32_t max_batch, int32_t in_flight, int64_t table_budget_bytes,
                           int64_t result_budget_bytes);
 /* Waits for the queries in flight, stops the scheduler and frees everything (tickets included). */

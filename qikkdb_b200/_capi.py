@@ -96,7 +96,7 @@ class qdb_server_result(C.Structure):
 
 class qdb_server_stats(C.Structure):
     _fields_ = [(f, C.c_int64) for f in ("submitted", "completed", "batches", "retries", "rejected",
-                                         "queries_in_batches")]
+                                         "queries_in_batches", "table_budget_bytes", "hbm_free_at_create")]
 
 
 P = C.c_void_p
@@ -156,6 +156,7 @@ SIGNATURES = [
     ("qdb_gb_batch_required", I32, [C.POINTER(qdb_gb_query), I32, PI64, PI64]),
     ("qdb_gb_batch_set_sharing", I32, [P, I32]),
     ("qdb_gb_batch_tuning_reset", I32, []),
+    ("qdb_gb_plain_run", I32, [C.POINTER(qdb_gb_query), I32, I32, PI64, P]),
     ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
     ("qdb_server_destroy", I32, [P]),
     ("qdb_server_submit", I32, [P, C.POINTER(qdb_gb_query), C.POINTER(C.c_uint64)]),

@@ -188,5 +188,16 @@ def required_bytes(queries: Sequence[Query]) -> tuple:
     return t.value, r.value
 
 
+def plain_run(queries: Sequence[Query], results_to_host: bool = True, stream=None) -> np.ndarray:
+    """The same queries one at a time through the plain path, looped in C (qdb_gb_plain_run): per query the
+    `key % key_mod` column, a table, ProcessBlock with the fused WHERE, GetResults, optionally the results copied to
+    host memory, then everything freed.  Returns every query's group count."""
+    arr = (capi.qdb_gb_query * max(len(queries), 1))(*[q.to_c() for q in queries])
+    groups = np.zeros(max(len(queries), 1), np.int64)
+    capi.check(capi.lib().qdb_gb_plain_run(arr, len(queries), 1 if results_to_host else 0,
+                                           groups.ctypes.data_as(C.POINTER(C.c_int64)), _stream(stream)))
+    return groups[:len(queries)]
+
+
 def tuning_reset() -> None:
     capi.check(capi.lib().qdb_gb_batch_tuning_reset())

@@ -839,4 +839,58 @@ int32_t qdb_gb_batch_tuning_reset(void) {
     return QDB_OK;
 }
 
+int32_t qdb_gb_plain_run(const qdb_gb_query* queries, int32_t n, int32_t results_to_host, int64_t* out_groups,
+                         void* stream) {
+    if (n < 0 || (n > 0 && !queries)) return fail(QDB_ERR_INVALID, "qdb_gb_plain_run: bad arguments");
+    static const int32_t kAggOrder[5] = {QDB_AGG_MIN, QDB_AGG_MAX, QDB_AGG_SUM, QDB_AGG_AVG, QDB_AGG_COUNT};
+    std::vector<int64_t> host;
+    for (int32_t i = 0; i < n; ++i) {
+        const qdb_gb_query& q = queries[i];
+        if (out_groups) out_groups[i] = 0;
+        const int32_t ks = type_size(q.key_type);
+        if (ks == 0 || q.n_rows < 0) return fail(QDB_ERR_INVALID, "qdb_gb_plain_run: bad query");
+        // GROUP BY key % m: the dispatcher materialises the modulo column first (GPUBinary<mod>).
+        const void* key = q.keys;
+        void* modcol = nullptr;
+        int32_t rc = QDB_OK;
+        if (q.key_mod > 0 && q.n_rows > 0) {
+            rc = qdb_malloc(&modcol, q.n_rows * ks, stream);
+            if (rc == QDB_OK) rc = qdb_arith_mod(q.key_type, q.keys, q.key_mod, modcol, q.n_rows, stream);
+            key = modcol;
+        }
+        qdb_gb* gb = nullptr;
+        if (rc == QDB_OK)
+            rc = qdb_gb_create(&gb, q.agg_mask, q.key_type, 1, q.val_type, q.max_groups, QDB_PLACE_AUTO, stream);
+        if (rc == QDB_OK) {
+            const void* kc[1] = {key};
+            rc = qdb_gb_process_sync(gb, kc, nullptr, q.vals, nullptr, q.n_rows, q.pred.col ? &q.pred : nullptr,
+                                     nullptr, stream);
+        }
+        int32_t aggs[5];
+        int32_t na = 0;
+        for (int32_t b : kAggOrder)
+            if (q.agg_mask & b) aggs[na++] = b;
+        void* okeys[1] = {nullptr};
+        void* ovals[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        int64_t g = 0;
+        if (rc == QDB_OK) rc = qdb_gb_results_multi(gb, na, aggs, okeys, nullptr, ovals, nullptr, &g, stream);
+        if (rc == QDB_OK && results_to_host && g > 0) {
+            // keys, then every aggregate column (COUNT int64, the others of the value type) to host memory
+            host.resize(static_cast<size_t>(g) * (1 + na));
+            rc = qdb_memcpy_d2h(host.data(), okeys[0], g * ks, stream);
+            for (int32_t j = 0; j < na && rc == QDB_OK; ++j) {
+                const int64_t w = aggs[j] == QDB_AGG_COUNT ? 8 : type_size(q.val_type);
+                rc = qdb_memcpy_d2h(host.data() + static_cast<size_t>(g) * (1 + j), ovals[j], g * w, stream);
+            }
+        }
+        qdb_free(okeys[0], stream);
+        for (void* v : ovals) qdb_free(v, stream);
+        if (gb) qdb_gb_destroy(gb);
+        qdb_free(modcol, stream);
+        if (rc != QDB_OK) return rc;
+        if (out_groups) out_groups[i] = g;
+    }
+    return qdb_stream_sync(stream);
+}
+
 }  // extern "C"

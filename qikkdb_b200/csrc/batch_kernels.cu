@@ -445,7 +445,7 @@ __device__ void b_tile(const BInst& I, const unsigned char* st, int koff, int vo
             bool pend[RPT];
 #pragma unroll
             for (int u = 0; u < RPT; ++u) {
-                pos[u] = mix64(kw[u]) & main.mask;
+                pos[u] = home_slot(main, mix64(kw[u]));
                 pend[u] = ok[u] && kw[u] != kEmpty;
                 slot[u] = nullptr;
                 cur[u] = pend[u] ? ld_volatile_u64(main.slots + pos[u] * W) : 0ull;

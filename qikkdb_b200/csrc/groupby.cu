@@ -376,18 +376,35 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
         return (o + 127) & ~size_t(127);
     };
 
-    // Spill plan: partitions small enough for the spill pass's table (50 KB: four CTAs per SM) at half load.
+    // Spill plan: partitions small enough for the spill pass's table (one CTA per SM, the largest table shared
+    // memory holds after the cell-fill prefix and the second-level counters) at half load.  The aggregation pass
+    // writes at most 2^kMaxSpillBits partitions (its (partition, CTA) cells then fit L2, which combines their partly
+    // written sectors); a table needing more has two levels: the spill pass over the first level aggregates what its
+    // table takes and sends the other rows to 2^spill_bits2 sub-partitions per partition, which a third pass
+    // aggregates.
     int spill_bits = -1;
+    int spill_bits2 = 0;
     int NB2 = 0;
+    const int64_t ctas_plan = std::min<int64_t>(di.sm_count, (a.n + kFastT - 1) / kFastT);
+    const size_t prefix2 = ((static_cast<size_t>(ctas_plan) + 1) * 4 + 127) / 128 * 128;
+    const size_t fill2_bytes = (size_t(4) << kMaxSpill2Bits);
     {
-        const size_t budget2 = static_cast<size_t>(env_int("QDB_SPILL_SMEM_KB", 50)) * 1024 - 1024;  // - the fill prefix
+        const int64_t kb = env_int("QDB_SPILL_SMEM_KB", 0);
+        const size_t budget2 = (kb > 0 ? static_cast<size_t>(kb) * 1024 : static_cast<size_t>(di.max_smem_optin) - 1024) -
+                               prefix2 - fill2_bytes;
         NB2 = static_cast<int>(budget2 / bucket_bytes);
         if (NB2 >= 64 && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
             const uint64_t per = static_cast<uint64_t>(NB2);  // distinct keys per partition at half load
             const uint64_t parts = next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per);
             int bits = 0;
             while ((1ull << bits) < parts) ++bits;
-            if (bits <= 10) spill_bits = bits;
+            const int max1 = static_cast<int>(env_int("QDB_SPILL_BITS_MAX", kMaxSpillBits));
+            if (bits <= max1) {
+                spill_bits = bits;
+            } else if (bits <= max1 + kMaxSpill2Bits && int64_t(1) << max1 >= di.sm_count) {
+                spill_bits = max1;
+                spill_bits2 = bits - max1;
+            }
         }
     }
     const size_t bar_bytes = 128;
@@ -410,6 +427,7 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
     a.fits = fits ? 1 : 0;
     a.probe_b = fits ? 8 : 1;
     a.dedup = static_cast<int32_t>(env_int("QDB_DEDUP", 2));
+    a.flush_rounds = static_cast<int32_t>(env_int("QDB_FLUSH_ROUNDS", 16));
     a.T = kFastT;
     a.NS = NS;
     a.sl = sl;
@@ -419,16 +437,20 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
 
     SpillArea* spill = nullptr;
     if (spill_bits >= 0) {
-        // One cell per (partition, CTA), each holding 5/4 of its share of half this call's rows (at most 2^28 rows in
-        // all) plus 64: warps whose hit rate is below 1/2 stop spilling, and rows of a full cell go to the global table.
+        // One cell per (partition, CTA), each holding 5/4 of its share of this call's rows (at most 2^29 rows in all)
+        // plus 64; rows of a full cell go to the global table.
         const int64_t parts = int64_t(1) << spill_bits;
         const int64_t ctas = std::min<int64_t>(di.sm_count, a.tiles);
-        const int64_t rows = std::min<int64_t>((a.n + 1) / 2, int64_t(1) << 28);
-        const int64_t cell = (rows + rows / 4) / (parts * ctas) + 64;
+        const int64_t rows = std::min<int64_t>(a.n + a.n / 4, int64_t(1) << 29);
+        const int64_t cell = rows / (parts * ctas) + 64;
         // Records of 16 bytes (key word, value bits), or 8 (the key word) for a count-only table; one more fill word
         // is the spill pass's work counter.
         const uint64_t words = static_cast<uint64_t>(parts * ctas * cell) * (vs ? 2 : 1);
-        int32_t rc = spill_acquire(gb->device, words, 0, parts * ctas + 1, s, &spill);
+        // A second level takes as many records again, in 2^spill_bits2 cells per first-level partition, and its own
+        // fill words (plus the third pass's work counter).
+        const int64_t cells2 = spill_bits2 ? (parts << spill_bits2) : 0;
+        int32_t rc = spill_acquire(gb->device, spill_bits2 ? 2 * words : words, 0,
+                                   parts * ctas + 1 + (spill_bits2 ? cells2 + 1 : 0), s, &spill);
         if (rc != QDB_OK) return rc;
         a.spill_keys = spill->keys;
         a.spill_vals = nullptr;
@@ -436,6 +458,12 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
         a.spill_cell = cell;
         a.spill_bits = spill_bits;
         a.spill_ctas = static_cast<int32_t>(ctas);
+        if (spill_bits2) {
+            a.spill2_keys = spill->keys + words;
+            a.spill2_fill = spill->fill + parts * ctas + 1;
+            a.spill2_cell = ctas * cell >> spill_bits2;
+            a.spill2_bits = spill_bits2;
+        }
     }
     a.so_bar = static_cast<int32_t>(tab_bytes);
     a.so_list = static_cast<int32_t>(tab_bytes + bar_bytes);
@@ -448,19 +476,36 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
         if (spill) spill_release(spill, s);
         return rc;
     }
-    // Spill pass: partitions x slices CTAs, each with a table of NB2 buckets.
+    // Spill pass: one persistent CTA per SM, each with a table of NB2 buckets, taking (partition, slice) items; a
+    // partition is cut into slices only when there are fewer partitions than CTAs.  Over the first of two levels the
+    // table takes a key only into its home bucket and sends the rest on; the last level's table takes every key.
     AggArgs b = a;
     const size_t tab2 = layout_table(b, NB2);
     b.so_spill = static_cast<int32_t>(tab2);  // the prefix of the cell fills
-    const size_t smem2 = tab2 + ((static_cast<size_t>(a.spill_ctas) + 1) * 4 + 127) / 128 * 128;
-    b.fits = 1;
-    b.probe_b = 8;
-    // Persistent CTAs (four per SM) take (partition, slice) items; a partition is cut into slices only when there are
-    // fewer partitions than CTAs.
+    b.so_spill2 = static_cast<int32_t>(tab2 + prefix2);
+    const size_t smem2 = tab2 + prefix2 + fill2_bytes;
+    b.fits = spill_bits2 ? 0 : 1;
+    b.probe_b = spill_bits2 ? 1 : 8;
     const int64_t parts = int64_t(1) << spill_bits;
-    const int64_t ctas2 = 4 * static_cast<int64_t>(di.sm_count);
+    const int64_t ctas2 = static_cast<int64_t>(di.sm_count);
     const int64_t slices = std::max<int64_t>(1, std::min<int64_t>(a.spill_ctas, ctas2 / parts));
     rc = launch_fspill(gb, b, smem2, std::min<int64_t>(ctas2, parts * slices), static_cast<int32_t>(slices), s);
+    if (rc == QDB_OK && spill_bits2) {
+        // Third pass: every second-level cell is one partition of 2^(spill_bits + spill_bits2).
+        AggArgs c = b;
+        c.spill_keys = a.spill2_keys;
+        c.spill_fill = a.spill2_fill;
+        c.spill_cell = a.spill2_cell;
+        c.spill_bits = spill_bits + spill_bits2;
+        c.spill_ctas = 1;
+        c.spill2_keys = nullptr;
+        c.spill2_fill = nullptr;
+        c.spill2_bits = 0;
+        c.fits = 1;
+        c.probe_b = 8;
+        const int64_t items3 = int64_t(1) << c.spill_bits;
+        rc = launch_fspill(gb, c, smem2, std::min<int64_t>(ctas2, items3), 1, s);
+    }
     spill_release(spill, s);
     return rc;
 }

@@ -102,6 +102,15 @@ struct AggArgs {
     int32_t probe_b = 1;   // buckets a claim may visit
     int32_t dedup = 2;     // warp aggregation of equal keys: 0 off, 1 on, 2 decided per warp from its first batches
     int32_t pred_float = 0;  // the fast pass compares IEEE predicate values as order-preserving integers
+    int32_t flush_rounds = 16;  // lock-step probe rounds of a shared table's merge into the global table
+    // Second spill level (fast pass, tables with more partitions than one pass writes well): the spill pass over the
+    // first level sends the rows its table cannot take to cell p * 2^spill2_bits + q of this area, q the next
+    // spill2_bits bits of the key's hash, and a third pass aggregates those cells.
+    uint64_t* spill2_keys = nullptr;
+    uint32_t* spill2_fill = nullptr;  // [2^(spill_bits + spill2_bits)] rows per cell, then the next pass's work counter
+    int64_t spill2_cell = 0;
+    int32_t spill2_bits = 0;
+    int32_t so_spill2 = 0;            // shared-memory offset of the spill pass's second-level fill counters
 };
 
 template <typename A, typename B>
@@ -235,7 +244,12 @@ __device__ __forceinline__ long long enc64(VT v) {
 // New groups are counted in a per-CTA shared-memory counter (a single global counter hit by every new
 // key would serialise in L2); each CTA publishes its count once with publish_claims, which raises
 // HASH_TABLE_FULL when the total passes the capacity.
-__device__ __forceinline__ void claim_counted(unsigned long long* claims) { atomicAdd(claims, 1ull); }
+// A CTA claims fewer than 2^32 groups per launch, so the count lives in the low 32-bit word of its 64-bit counter
+// and a native 32-bit shared atomic updates it: a 64-bit shared atomic is a retry loop, which collapses when a
+// thousand threads claim new groups at once (the spill pass merging a partition of new keys).
+__device__ __forceinline__ void claim_counted(unsigned long long* claims) {
+    atomicAdd(reinterpret_cast<unsigned int*>(claims), 1u);
+}
 
 __device__ __forceinline__ void publish_claims(unsigned long long* counters, unsigned long long capacity,
                                                unsigned long long claims) {
@@ -272,9 +286,14 @@ __device__ __forceinline__ uint64_t* g_find_from(const Region& R, int W, uint64_
     return nullptr;
 }
 
+// Home slot of a key whose mix64 hash is h: the top log2(cap) bits of h.  A key's spill partition (fast pass) is the
+// top bits of the same hash, so the groups of one partition live in one contiguous stretch of the table and the
+// spill pass's merge of a partition touches that stretch only.
+__device__ __forceinline__ uint64_t home_slot(const Region& R, uint64_t h) { return __umul64hi(h, R.mask + 1); }
+
 __device__ __forceinline__ uint64_t* g_find(const Region& R, int W, uint64_t key, uint64_t h,
                                             unsigned long long* counters, unsigned long long* claims) {
-    const uint64_t s = h & R.mask;
+    const uint64_t s = home_slot(R, h);
     return g_find_from(R, W, key, s, ld_volatile_u64(R.slots + s * W), counters, claims);
 }
 
@@ -685,7 +704,7 @@ __device__ __forceinline__ void s_flush(const STable& t, const AggArgs& a, int S
         for (int u = 0; u < U; ++u) {
             const int i = i0 + u * blockDim.x;
             key[u] = (i < S) ? t.key[i] : kEmpty;
-            pos[u] = mix64(key[u]) & a.main.mask;
+            pos[u] = home_slot(a.main, mix64(key[u]));
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) cur[u] = (key[u] != kEmpty) ? ld_volatile_u64(a.main.slots + pos[u] * W) : 0ull;

@@ -35,6 +35,8 @@ constexpr int kFastR = 32 * kFastSeg;               // rows per warp and tile
 constexpr int kFastT = kFastWarps * kFastR;         // rows per tile (2048)
 constexpr int kDedupTrial = 4;                      // steps a warp runs with warp aggregation before deciding
 constexpr int kDedupGroup = 4;                      // lanes sharing a slot that are combined before the update
+constexpr int kMaxSpillBits = 10;                   // partitions the aggregation pass writes: at most 1024
+constexpr int kMaxSpill2Bits = 6;                   // second-level partitions per first-level one: at most 64
 constexpr uint64_t kHashMul = 0x9E3779B97F4A7C15ull;
 
 __device__ __forceinline__ uint32_t atoms_or(uint32_t a, uint32_t x) {
@@ -65,9 +67,10 @@ __device__ __forceinline__ FTab ftab(unsigned char* sm, const AggArgs& a) {
     return t;
 }
 
-// Hash of a key word: one 64-bit multiply (Fibonacci hashing, Knuth TAOCP vol. 3, 6.4).  The top bits pick the spill
-// partition, the 32 bits below bit `shift` (32 - partition bits) the bucket, and bits 32..46 the bit of the seen-once
-// filter.
+// Hash of a key word for the shared tables: one 64-bit multiply (Fibonacci hashing, Knuth TAOCP vol. 3, 6.4).  Its
+// top 32 bits pick the bucket and bits 32..46 the bit of the seen-once filter.  The spill partition comes from the
+// independent mix64 hash (the global table's), so a partition's rows spread over every bucket of the spill pass's
+// table.
 __device__ __forceinline__ uint64_t fhash(uint64_t kw) { return kw * kHashMul; }
 __device__ __forceinline__ uint32_t fbucket(uint64_t m, int shift, uint32_t NB) {
     const uint32_t x = __funnelshift_rc(static_cast<uint32_t>(m), static_cast<uint32_t>(m >> 32), shift);
@@ -194,8 +197,12 @@ __device__ __forceinline__ void ftab_init(unsigned char* sm, const AggArgs& a, i
     }
 }
 
-// Merges every occupied slot into the global table (whole CTA).  Each thread takes four slots at a time and issues the
-// four home-slot loads of the global table before resolving any of them, so the L2 round trips overlap.
+// Merges every occupied slot into the global table (whole CTA).  Each thread takes U slots at a time and finds their
+// global slots in lock-step rounds: a round issues the pending probe loads, or the claims (CAS) of keys that met an
+// empty slot, of all U before it looks at any result, so their L2/DRAM round trips overlap.  A key still unresolved
+// after a.flush_rounds rounds (a long probe run) finishes with the one-key search, which bounds the probe and reports
+// a full table.
+
 template <typename VT>
 __device__ __forceinline__ void ftab_flush(unsigned char* sm, const AggArgs& a, const FixQ& fq,
                                            unsigned long long* claims) {
@@ -208,26 +215,54 @@ __device__ __forceinline__ void ftab_flush(unsigned char* sm, const AggArgs& a, 
     const unsigned* l0 = reinterpret_cast<const unsigned*>(sm + a.so_l0);
     const unsigned* l1 = reinterpret_cast<const unsigned*>(sm + a.so_l1);
     const unsigned char* mm = sm + a.so_mn;
+    const uint64_t mask = a.main.mask;
     constexpr int U = 4;
     for (int i0 = threadIdx.x; i0 < S; i0 += U * blockDim.x) {
         uint64_t key[U], pos[U], cur[U];
+        uint64_t* g[U];
+        bool pend[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int i = i0 + u * blockDim.x;
-            key[u] = (i < S) ? keys[i] : kEmpty;
-            pos[u] = mix64(key[u]) & a.main.mask;
+            const int ki = i0 + u * blockDim.x;
+            key[u] = (ki < S) ? keys[ki] : kEmpty;
+            g[u] = nullptr;
+            pend[u] = key[u] != kEmpty && cnt[(ki & 1) * a.NB + (ki >> 1)] != 0u;  // key index 2 b + j -> state j NB + b
+            pos[u] = pend[u] ? home_slot(a.main, mix64(key[u])) : 0ull;
         }
 #pragma unroll
-        for (int u = 0; u < U; ++u) cur[u] = (key[u] != kEmpty) ? ld_volatile_u64(a.main.slots + pos[u] * W) : 0ull;
+        for (int u = 0; u < U; ++u) cur[u] = pend[u] ? ld_volatile_u64(a.main.slots + pos[u] * W) : 0ull;
+        for (int r = 0; r < a.flush_rounds && (pend[0] | pend[1] | pend[2] | pend[3]); ++r) {
+            unsigned long long prev[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)  // claims of keys that met an empty slot, all issued before any is read
+                prev[u] = (pend[u] && cur[u] == kEmpty)
+                              ? atomicCAS(reinterpret_cast<unsigned long long*>(a.main.slots + pos[u] * W), kEmpty, key[u])
+                              : cur[u];
+            bool load[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                load[u] = false;
+                if (!pend[u]) continue;
+                if (prev[u] == key[u] || (cur[u] == kEmpty && prev[u] == kEmpty)) {
+                    if (cur[u] == kEmpty && prev[u] == kEmpty) claim_counted(claims);
+                    g[u] = a.main.slots + pos[u] * W;
+                    pend[u] = false;
+                } else {  // the slot holds another key: probe the next one
+                    pos[u] = (pos[u] + 1) & mask;
+                    load[u] = true;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (load[u]) cur[u] = ld_volatile_u64(a.main.slots + pos[u] * W);
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            if (key[u] == kEmpty) continue;
+            if (pend[u]) g[u] = g_find_from(a.main, W, key[u], pos[u], cur[u], a.counters, claims);
+            if (!g[u]) continue;
             const int ki = i0 + u * blockDim.x;
-            const int i = (ki & 1) * a.NB + (ki >> 1);  // key index 2 b + j -> state index j NB + b
+            const int i = (ki & 1) * a.NB + (ki >> 1);
             const unsigned long long c = cnt[i];
-            if (c == 0) continue;
-            uint64_t* g = g_find_from(a.main, W, key[u], pos[u], cur[u], a.counters, claims);
-            if (!g) continue;
             uint64_t sumbits = 0;
             if (a.has_sum) {
                 const uint64_t s = (static_cast<uint64_t>(l1[i]) << 32) | l0[i];
@@ -250,7 +285,7 @@ __device__ __forceinline__ void ftab_flush(unsigned char* sm, const AggArgs& a, 
                     mx = w[1];
                 }
             }
-            g_merge(g, a.L, a.has_sum, a.has_min, a.has_max, V32, VFLOAT, c, sumbits, mn, mx);
+            g_merge(g[u], a.L, a.has_sum, a.has_min, a.has_max, V32, VFLOAT, c, sumbits, mn, mx);
         }
     }
 }
@@ -283,10 +318,17 @@ struct FastWarp {
     int trial = 0;         // steps run so far in the warp-aggregation trial
     unsigned trial_hits = 0, trial_leaders = 0;  // warp totals over the trial
     unsigned hits = 0, tries = 0;
-    // spill addressing of this CTA (aggregation pass only)
+    // Where a miss goes: partition q = (mix64(key) >> part_shift) & part_mask, appended to cell cell_base + q cell_mul
+    // of spill_out (records of 16 bytes, or 8 for a count-only table) at the position its shared fill counter
+    // sfill[q] hands out; a full cell sends the row to the global table.
     uint32_t sfill = 0;    // shared-window address of the per-partition fill counters
     uint32_t seen = 0;     // shared-window address of the seen-once filter (0: admit every key)
     unsigned cell_cap = 0;
+    int part_shift = 64;
+    uint32_t part_mask = 0;
+    int64_t cell_base = 0;
+    int64_t cell_mul = 0;
+    uint64_t* spill_out = nullptr;
 
     __device__ __forceinline__ FastWarp(const AggArgs& args, const FTab& tab, const FixQ& f, unsigned long long* c)
         : a(args), t(tab), fq(f), claims(c) {}
@@ -381,19 +423,20 @@ struct FastWarp {
     }
 
     // A row the shared table did not take: appended to its partition's spill cell, or inserted into the global table.
-    __device__ __forceinline__ void miss_row(uint64_t kw, VT v, uint64_t m, bool spillable) {
+    __device__ __forceinline__ void miss_row(uint64_t kw, VT v, bool spillable) {
         if (spill_ok && spillable) {
-            const uint32_t p = a.spill_bits ? (static_cast<uint32_t>(m >> 32) >> (32 - a.spill_bits)) : 0u;
+            // The partition comes from the key's mix64 hash, whose top bits are its home slot in the global table.
+            const uint32_t p = part_shift < 64 ? static_cast<uint32_t>(mix64(kw) >> part_shift) & part_mask : 0u;
             const unsigned pos = atoms_add(sfill + p * 4u, 1u);
             if (pos < cell_cap) {
                 // One record per row (key word, value bits): a single 8- or 16-byte store.
-                const uint64_t idx = static_cast<uint64_t>(p * static_cast<uint32_t>(a.spill_ctas) + blockIdx.x) * cell_cap + pos;
+                const uint64_t idx = static_cast<uint64_t>(cell_base + static_cast<int64_t>(p) * cell_mul) * cell_cap + pos;
                 if constexpr (VALS) {
                     uint64_t vb = 0;
                     memcpy(&vb, &v, sizeof(VT));
-                    reinterpret_cast<ulonglong2*>(a.spill_keys)[idx] = make_ulonglong2(kw, vb);
+                    reinterpret_cast<ulonglong2*>(spill_out)[idx] = make_ulonglong2(kw, vb);
                 } else {
-                    a.spill_keys[idx] = kw;
+                    spill_out[idx] = kw;
                 }
                 return;
             }
@@ -500,7 +543,7 @@ struct FastWarp {
         if (__any_sync(0xffffffffu, miss[0] | miss[1])) {
 #pragma unroll
             for (int u = 0; u < 2; ++u)
-                if (miss[u]) miss_row(kw[u], v[u], m[u], (kw[u] != kEmpty) & inwin[u]);
+                if (miss[u]) miss_row(kw[u], v[u], (kw[u] != kEmpty) & inwin[u]);
         }
     }
 };
@@ -636,6 +679,11 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
             fw.sfill = smem_u32(sfill);
             fw.seen = smem_u32(sfill + parts);
             fw.cell_cap = static_cast<unsigned>(a.spill_cell);
+            fw.part_shift = 64 - a.spill_bits;
+            fw.part_mask = static_cast<uint32_t>(parts - 1);
+            fw.cell_base = blockIdx.x;
+            fw.cell_mul = a.spill_ctas;
+            fw.spill_out = a.spill_keys;
         }
         auto pass = [&](PL x) -> bool { return ((x >= plo) & (x <= phi)) != pinv; };
         auto ring_row = [&](int g, uint64_t& kw, VT& v) {
@@ -762,17 +810,13 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                 s = 0;
                 ph ^= 1u;
             }
-            // After the table's fill phase a warp judges its hit rate.  Below 1/2 (keys spread evenly over many more
-            // groups than the table holds) the spill would carry most rows through HBM twice, which measured slower
-            // than inserting them into the global table directly; below 1/8 the warp also stops probing.
+            // After the table's fill phase a warp judges its hit rate: below 1/8 (keys spread evenly over many more
+            // groups than the table holds) it stops probing the table and sends every row to the spill, which the
+            // spill pass aggregates partition by partition in shared memory.
             if (q + 1 == kCountTile) fw.hits = fw.tries = 0;
             if (q == kDecideTile && fw.use_smem) {
                 const unsigned h = __reduce_add_sync(0xffffffffu, fw.hits);
                 const unsigned t = __reduce_add_sync(0xffffffffu, fw.tries);
-                if (t >= 256 && h * 2u < t) {
-                    fw.spill_ok = false;
-                    fw.seen = 0;
-                }
                 if (t >= 256 && h * 8u < t) fw.use_smem = false;
                 fw.counting = false;
             }
@@ -796,33 +840,44 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
 
 // ---------------------------------------------------------------------------------------------
 // Second pass over the spill.  Work item i is partition p = i % parts, slice j = i / parts: the cells j, j + slices, ...
-// of p (one per aggregation-pass CTA).  Persistent CTAs take items from a counter in global memory, aggregate the
-// item's rows in a bucketed shared table and merge it into the global table.  The cells' records are read as one
-// stream (a prefix of their fill counts maps a stream row to its cell), so every step but the last takes 64 rows
-// however small the cells are, and each warp loads its next step's records before it processes the current one.
+// of p (one per aggregation-pass CTA).  One persistent CTA per SM takes items from a counter in global memory,
+// aggregates the item's rows in a bucketed shared table as large as shared memory allows and merges it into the
+// global table.  The item's cells are read as one stream (a prefix of their fill counts maps a stream row to its
+// cell): warp w takes the contiguous stream range [total w / W, total (w + 1) / W), finds the cell of its first row
+// once and then moves its cell cursor forward step by step, so every step but the last takes 64 rows however small
+// the cells are, and each warp loads its next step's records before it processes the current one.
 // ---------------------------------------------------------------------------------------------
+constexpr int kFSpillThreads = 1024;
+
 template <typename VT, int MODE>
-__global__ void __launch_bounds__(kSpillThreads) gb_fspill_kernel(const AggArgs a, int32_t slices) {
+__global__ void __launch_bounds__(kFSpillThreads, 1) gb_fspill_kernel(const AggArgs a, int32_t slices) {
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ unsigned long long s_claims;
     __shared__ int s_emax;
     __shared__ int s_item;
     constexpr bool VFLOAT = std::is_floating_point<VT>::value;
     constexpr bool VALS = (MODE & FM_VALS) != 0;
-    constexpr int kWarps = kSpillThreads / 32;
+    constexpr int kWarps = kFSpillThreads / 32;
     const FTab tab = ftab(sm, a);
     const int parts = 1 << a.spill_bits;
     const int items = parts * slices;
     unsigned* work = a.spill_fill + static_cast<int64_t>(parts) * a.spill_ctas;  // zeroed by the aggregation pass
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* pre = reinterpret_cast<int*>(sm + a.so_spill);  // pre[t]: rows of the item's cells before its t-th cell
+    // First level of a two-level spill: the rows this pass's table cannot take go to the second level.
+    const bool level2 = a.spill2_keys != nullptr;
+    const int parts2 = level2 ? (1 << a.spill2_bits) : 0;
+    unsigned* fill2 = reinterpret_cast<unsigned*>(sm + a.so_spill2);
     if (threadIdx.x == 0) s_claims = 0;
+    if (level2 && blockIdx.x == 0 && threadIdx.x == 0)
+        a.spill2_fill[static_cast<int64_t>(parts) * parts2] = 0u;  // the next pass's work counter
     for (;;) {
         if (threadIdx.x == 0) {
             s_item = static_cast<int>(atomicAdd(work, 1u));
             s_emax = INT_MIN;
             pre[0] = 0;
         }
+        for (int i = threadIdx.x; i < parts2; i += blockDim.x) fill2[i] = 0u;
         ftab_init<VT>(sm, a, threadIdx.x, blockDim.x);
         __syncthreads();
         const int item = s_item;
@@ -853,32 +908,33 @@ __global__ void __launch_bounds__(kSpillThreads) gb_fspill_kernel(const AggArgs 
         }
         __syncthreads();
         const int total = pre[ncells];
-        auto rec = [&](int r, int t) -> int64_t {  // spill row of stream row r, which lies in the item's t-th cell
-            return (cell0 + j + static_cast<int64_t>(slices) * t) * a.spill_cell + (r - pre[t]);
-        };
-        // The step starting at stream row r0 (two rows per lane): cells, then the records.
-        auto load = [&](int r0, bool (&act)[2], uint64_t (&kw)[2], VT (&v)[2]) {
-            int lo = 0, hi = ncells;  // the cell of r0: the largest t with pre[t] <= r0
+        const int r_end = static_cast<int>(static_cast<int64_t>(total) * (warp + 1) / kWarps);
+        int r0 = static_cast<int>(static_cast<int64_t>(total) * warp / kWarps);
+        // The warp's cell cursor: the largest t with pre[t] <= r0 (pre[0] = 0 <= r0; empty cells share a prefix).
+        int tw = 0;
+        {
+            int lo = 0, hi = ncells;
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (pre[mid] <= r0) lo = mid;
                 else hi = mid;
             }
-            int t[2] = {lo, lo};
-            const int r[2] = {r0 + lane, r0 + 32 + lane};
-            for (int tb = lo + 1; tb < ncells && pre[tb] < r0 + 64; ++tb) {  // cells that start inside the step
-                const int B = pre[tb];
-#pragma unroll
-                for (int u = 0; u < 2; ++u)
-                    if (r[u] >= B) t[u] = tb;
-            }
+            tw = lo;
+        }
+        // The step starting at stream row s0 (two rows per lane, s0 + lane and s0 + 32 + lane): moves the cursor to
+        // the cell of s0, then each lane walks forward to the cell of its own rows and loads their records.
+        auto load = [&](int s0, bool (&act)[2], uint64_t (&kw)[2], VT (&v)[2]) {
+            while (tw + 1 < ncells && pre[tw + 1] <= s0) ++tw;
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
-                act[u] = r[u] < total;
+                const int r = s0 + 32 * u + lane;
+                act[u] = r < r_end;
                 kw[u] = 0ull;
                 v[u] = VT{};
                 if (act[u]) {
-                    const int64_t ri = rec(r[u], t[u]);
+                    int t = tw;
+                    while (t + 1 < ncells && pre[t + 1] <= r) ++t;
+                    const int64_t ri = (cell0 + j + static_cast<int64_t>(slices) * t) * a.spill_cell + (r - pre[t]);
                     if constexpr (VALS) {
                         const ulonglong2 x = reinterpret_cast<const ulonglong2*>(a.spill_keys)[ri];
                         kw[u] = x.x;
@@ -889,11 +945,12 @@ __global__ void __launch_bounds__(kSpillThreads) gb_fspill_kernel(const AggArgs 
                 }
             }
         };
-        if (VFLOAT && (MODE & FM_SUM)) {  // scale from the first rows of the stream
-            bool act[2];
-            uint64_t kw[2];
-            VT v[2];
-            load(warp * 64, act, kw, v);
+        bool act[2], nact[2];
+        uint64_t kw[2], nkw[2];
+        VT v[2], nv[2];
+        if (r0 < r_end) load(r0, act, kw, v);
+        else act[0] = act[1] = false;
+        if (VFLOAT && (MODE & FM_SUM)) {  // fixed-point scale from every warp's first rows
             int e = max(act[0] ? fexp<VT>(v[0]) : INT_MIN, act[1] ? fexp<VT>(v[1]) : INT_MIN);
             e = __reduce_max_sync(0xffffffffu, e);
             if (lane == 0 && e != INT_MIN) atomicMax(&s_emax, e);
@@ -902,18 +959,23 @@ __global__ void __launch_bounds__(kSpillThreads) gb_fspill_kernel(const AggArgs 
         const int hb = max(1, 64 - __clzll(static_cast<long long>(total)));
         const FixQ fq = fixq<VT>(s_emax == INT_MIN ? 0 : s_emax, hb);
         FastWarp<VT, MODE> fw(a, tab, fq, &s_claims);
-        fw.bshift = 32 - a.spill_bits;
-        fw.fits = true;
+        fw.bshift = 32;
+        fw.fits = a.fits != 0;
         fw.probe_b = a.probe_b;
         fw.dedup = a.dedup != 0;
-        bool act[2], nact[2];
-        uint64_t kw[2], nkw[2];
-        VT v[2], nv[2];
-        int r0 = warp * 64;
-        if (r0 < total) load(r0, act, kw, v);
-        for (; r0 < total; r0 += kWarps * 64) {
-            const int n0 = r0 + kWarps * 64;
-            if (n0 < total) load(n0, nact, nkw, nv);
+        if (level2) {
+            fw.spill_ok = true;
+            fw.sfill = smem_u32(fill2);
+            fw.cell_cap = static_cast<unsigned>(a.spill2_cell);
+            fw.part_shift = 64 - a.spill_bits - a.spill2_bits;
+            fw.part_mask = static_cast<uint32_t>(parts2 - 1);
+            fw.cell_base = static_cast<int64_t>(p) * parts2;
+            fw.cell_mul = 1;
+            fw.spill_out = a.spill2_keys;
+        }
+        for (; r0 < r_end; r0 += 64) {
+            const int n0 = r0 + 64;
+            if (n0 < r_end) load(n0, nact, nkw, nv);
             fw.rows2(act, kw, v, static_cast<unsigned>(lane));
 #pragma unroll
             for (int u = 0; u < 2; ++u) {
@@ -923,6 +985,8 @@ __global__ void __launch_bounds__(kSpillThreads) gb_fspill_kernel(const AggArgs 
             }
         }
         __syncthreads();
+        for (int i = threadIdx.x; i < parts2; i += blockDim.x)
+            a.spill2_fill[static_cast<int64_t>(p) * parts2 + i] = min(fill2[i], static_cast<unsigned>(a.spill2_cell));
         ftab_flush<VT>(sm, a, fq, &s_claims);
         __syncthreads();
     }
@@ -956,7 +1020,7 @@ int32_t launch_fspill_t(const AggArgs& a, size_t smem, int64_t grid, int32_t sli
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(gb_fspill_kernel)");
     }
-    kern<<<static_cast<unsigned>(grid), kSpillThreads, smem, st>>>(a, slices);
+    kern<<<static_cast<unsigned>(grid), kFSpillThreads, smem, st>>>(a, slices);
     note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "gb_fspill_kernel launch");

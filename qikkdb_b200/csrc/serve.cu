@@ -313,15 +313,26 @@ int32_t qdb_server_create(qdb_server** out, int32_t max_batch, int32_t in_flight
                           int64_t result_budget_bytes) {
     if (!out) return fail(QDB_ERR_INVALID, "qdb_server_create: null out");
     *out = nullptr;
-    if (max_batch < 1 || in_flight < 1 || in_flight > 8 || table_budget_bytes < in_flight ||
-        result_budget_bytes < in_flight)
+    if (max_batch < 1 || in_flight < 1 || in_flight > 8 || result_budget_bytes < in_flight)
         return fail(QDB_ERR_INVALID, "qdb_server_create: bad sizes");
+    // The tables are carved out of the HBM that is free when the server starts (the reference sizes its device
+    // allocators from cudaMemGetInfo, qikkDB/QueryEngine/Context.cu:58, CudaMemAllocator.cu:116): a reserve of an
+    // eighth of the free memory (at least 2 GiB) stays for the spill area, result copies and other allocations, and
+    // a table budget beyond what is left (or a budget <= 0, "all of it") is cut down to it.
+    size_t free_b = 0, total_b = 0;
+    QDB_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t reserve = std::max<int64_t>(int64_t(2) << 30, static_cast<int64_t>(free_b / 8));
+    const int64_t avail = static_cast<int64_t>(free_b) - reserve - result_budget_bytes;
+    if (avail < in_flight) return fail(QDB_ERR_NOMEM, "qdb_server_create: not enough free device memory");
+    if (table_budget_bytes <= 0 || table_budget_bytes > avail) table_budget_bytes = avail;
     qdb_server* sv = new qdb_server();
     cudaGetDevice(&sv->device);
     sv->max_batch = max_batch;
     sv->in_flight = in_flight;
     sv->slot_table_bytes = table_budget_bytes / in_flight;
     sv->slot_result_bytes = result_budget_bytes / in_flight;
+    sv->stats.table_budget_bytes = table_budget_bytes;
+    sv->stats.hbm_free_at_create = static_cast<int64_t>(free_b);
     sv->slots.resize(in_flight);
     int32_t rc = QDB_OK;
     for (Slot& sl : sv->slots) {
