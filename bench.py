@@ -65,7 +65,10 @@ def parse_args():
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the plain, composite, batched and served sub-workloads of the default run")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served"])
+    ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served", "plain", "composite"])
+    ap.add_argument("--composite-rows", type=int, default=1 << 27)
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="plain / composite on their own: skip the oracle leg (profiling runs)")
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="batched / served: queries of the one-by-one plain-path comparison (0 = all / 24)")
@@ -169,7 +172,7 @@ def measured_peak():
 def profiled_traffic():
     """DRAM bytes per launch of the aggregation kernel from the committed ncu summary, if present."""
     try:
-        with open(os.path.join(ROOT, "profiles", "gb_agg_kernel_filtered_256M.json")) as f:
+        with open(os.path.join(ROOT, "profiles", "gb_fast_kernel_filtered_256M.json")) as f:
             d = json.load(f)
         return d.get("dram_bytes_per_launch_256M")
     except Exception:
@@ -481,10 +484,9 @@ def c0_measure(args, dev) -> dict:
 def c2_measure(args, dev) -> dict:
     import torch
 
-    import oracle
     from qikkdb_b200 import datagen as dg
     from qikkdb_b200.groupby import GroupByTable
-    n = 1 << 27
+    n = args.composite_rows
     aggs = ["sum", "count", "max"]
     a = dg.uniform_i32(C2_SEED, 0, n, 0, 4095)
     b = dg.uniform_i32(C2_SEED, 1, n, 0, 4095)
@@ -516,7 +518,10 @@ def c2_measure(args, dev) -> dict:
                         "frac": n * 16 / (kms / 1e3) / 1e9 / peak, "kernel_ms": kms,
                         "algorithmic_bytes_per_launch": n * 16, "peak_kind": peak_kind},
            "global_updates_per_s": n / (kms / 1e3)}
+    if getattr(args, "no_oracle", False):
+        return out
     # cpu_baseline leg: the oracle over every row, timed; its result checks the GPU result bit for bit
+    import oracle
     r = oracle.groupby([a, b], v, threads=0)
     out["cpu_baseline"] = {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
                            "sample": f"all {n} rows, hash-map GROUP BY, {r['threads']} threads, {r['seconds']:.1f} s"}
@@ -905,8 +910,22 @@ def run_served_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sub(args, fn):
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps(fn(args, torch.device("cuda", local))), flush=True)
+
+
 def main():
     args = parse_args()
+    if args.workload in ("plain", "composite"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the headline workload"}))
+            return
+        run_sub(args, c0_measure if args.workload == "plain" else c2_measure)
+        return
     if args.workload == "batched":
         if args.impl == "reference":
             run_batched_reference(args)

@@ -242,6 +242,25 @@ int32_t qdb_prefix_sum(const int8_t* mask, int64_t n, int32_t* out, void* stream
  * (newly allocated, ceil(n/64) words). */
 int32_t qdb_compress_null_mask(const uint8_t* in, int64_t n, uint64_t** out, void* stream);
 
+/* ---- ORDER BY over result columns: GPUOrderBy (qikkDB/QueryEngine/GPUCore/GPUOrderBy.cuh:88-195) ----
+ * qdb_order_by_column is one GPUOrderBy::OrderByColumn step: it re-sorts the permutation `indices` (n int32
+ * row numbers, device, caller-owned; first != 0 starts from the identity 0..n-1 instead of reading it) stably by
+ * the column `col` (qdb_type INT32, INT64, FLOAT or DOUBLE), ascending, or descending when descending != 0.  NULL
+ * rows (bits of the optional null mask) order as lowest(T), as the reference's TransformNullValsToSmallestVal makes
+ * them; floats order by their IEEE bits (-0.0 before +0.0), as a radix sort does.  Calling it for the ORDER BY
+ * columns from the last to the first, as the dispatcher does, leaves the lexicographic order with the first column
+ * most significant and ties in input order.  qdb_order_by does that for n_cols columns at once.
+ * qdb_reorder is ReOrderByIdx with OFFSET / LIMIT: out[i] = in[indices[offset + i]] for i < count;
+ * qdb_reorder_nulls is ReOrderNullValuesByIdx the same way (out holds ceil(count / 64) words).  Asynchronous. */
+int32_t qdb_order_by_column(int32_t type, const void* col, const uint64_t* nulls, int32_t descending, int64_t n,
+                            int32_t first, int32_t* indices, void* stream);
+int32_t qdb_order_by(int32_t n_cols, const int32_t* types, const void* const* cols, const uint64_t* const* nulls,
+                     const int32_t* descending, int64_t n, int32_t* out_indices, void* stream);
+int32_t qdb_reorder(int32_t elem_bytes, const void* in, const int32_t* indices, int64_t offset, int64_t count,
+                    void* out, void* stream);
+int32_t qdb_reorder_nulls(const uint64_t* in, const int32_t* indices, int64_t offset, int64_t count, uint64_t* out,
+                          void* stream);
+
 /* ---- batched GROUP BY: many independent queries in one persistent launch ----
  * The reference runs one GPUGroupBy per query, each with its own kernel launches and host synchronisations
  * (GpuSqlDispatcherAggregationFunctions.h:377-507 via GroupByHelper, :99-318).  A batch holds up to

@@ -9,6 +9,7 @@
  *   GPUBinary<FilterConditions::OP,int8_t,L,R>::Binary   GPUBinary.cuh:555-579
  *   GPUReconstruct::{reconstructColKeep, reconstructCol, GenerateIndexesKeep, GenerateIndexes, PrefixSum,
  *                    CompressNullMask}   GPUReconstruct.cuh:204-640
+ *   GPUOrderBy::{OrderByColumn, ReOrderByIdx, ReOrderNullValuesByIdx}   GPUOrderBy.cuh:88-195
  *   GPUMemory::{alloc, allocAndSet, free, copyHostToDevice, copyDeviceToHost, copyDeviceToDevice, memset}
  *                                          GPUMemory.cuh:18-236
  *   query_engine_error / gpu_error / QueryEngineErrorType   qikkDB/QueryEngine/GPUError.h:17-75
@@ -635,6 +636,62 @@ public:
         qdb_cpp::sync();
         return cuda_ptr<nullmask_t>(reinterpret_cast<nullmask_t*>(out));
     }
+};
+
+/* ---- ORDER BY over result columns: GPUOrderBy (GPUOrderBy.cuh:88-195, OrderByType.h, IOrderBy.h) ---- */
+namespace OrderBy {
+enum Order { ASC, DESC };
+}  // namespace OrderBy
+
+class IOrderBy {
+protected:
+    IOrderBy() = default;
+
+public:
+    virtual ~IOrderBy() = default;
+};
+
+/* The dispatcher creates one GPUOrderBy per result, calls OrderByColumn for the ORDER BY columns from the last to
+ * the first (each call re-sorts the kept permutation stably by one column; NULL rows order as lowest(T)), and
+ * reorders every result column and null mask by the indices. */
+class GPUOrderBy : public IOrderBy {
+public:
+    explicit GPUOrderBy(int32_t dataElementCount) : n_(dataElementCount > 0 ? dataElementCount : 0) {
+        GPUMemory::alloc(&indices_, n_ > 0 ? static_cast<size_t>(n_) : 1);
+    }
+    ~GPUOrderBy() override { qdb_free(indices_, nullptr); }
+    GPUOrderBy(const GPUOrderBy&) = delete;
+    GPUOrderBy& operator=(const GPUOrderBy&) = delete;
+
+    template <typename T>
+    void OrderByColumn(int32_t* outIndices, T* inCol, nullmask_t* nullBitMask, int32_t dataElementCount,
+                       OrderBy::Order order) {
+        qdb_cpp::check(qdb_order_by_column(qdb_cpp::type_of<T>::code, inCol, nullBitMask, order == OrderBy::DESC,
+                                           dataElementCount, first_ ? 1 : 0, indices_, nullptr));
+        first_ = false;
+        if (outIndices && dataElementCount > 0) GPUMemory::copyDeviceToDevice(outIndices, indices_, dataElementCount);
+        qdb_cpp::sync();
+    }
+
+    /* outCol[i] = inCol[inIndices[i]] (ReOrderByIdx, kernel_reorder_by_idx). */
+    template <typename T>
+    static void ReOrderByIdx(T* outCol, int32_t* inIndices, T* inCol, int32_t dataElementCount) {
+        qdb_cpp::check(qdb_reorder(static_cast<int32_t>(sizeof(T)), inCol, inIndices, 0, dataElementCount, outCol,
+                                   nullptr));
+        qdb_cpp::sync();
+    }
+
+    /* The null bits reordered the same way (ReOrderNullValuesByIdx). */
+    static void ReOrderNullValuesByIdx(nullmask_t* outNullBitMask, int32_t* indices, nullmask_t* inNullBitMask,
+                                       int32_t rowCount) {
+        qdb_cpp::check(qdb_reorder_nulls(inNullBitMask, indices, 0, rowCount, outNullBitMask, nullptr));
+        qdb_cpp::sync();
+    }
+
+private:
+    int32_t n_;
+    int32_t* indices_ = nullptr;
+    bool first_ = true;
 };
 
 #endif /* QDB_GROUPBY_HPP */

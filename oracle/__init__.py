@@ -50,6 +50,7 @@ def lib() -> C.CDLL:
         L.oracle_indexes.argtypes = [P, I64, P]
         L.oracle_prefix_sum.argtypes = [P, I64, P]
         L.oracle_reference_filter_inputs.argtypes = [I32, I32, I64, P, P]
+        L.oracle_order_by.argtypes = [I32, P, P, P, P, I64, P]
         _lib = L
     return _lib
 
@@ -137,6 +138,26 @@ def compact(col: np.ndarray, mask: np.ndarray, nulls=None):
     c = lib().oracle_compact(col.dtype.itemsize, _p(col), _p(np.ascontiguousarray(mask, dtype=np.int8)), len(col),
                              _p(out), _p(nulls), _p(nout))
     return out[:c], (nout if nout is not None else None), c
+
+
+def order_by(cols, descending=None, nulls=None) -> np.ndarray:
+    """Row permutation of ORDER BY cols[0], cols[1], ... (descending[c] per column; nulls[c] packed words or None)."""
+    cols = [np.ascontiguousarray(c) for c in cols]
+    n = len(cols[0])
+    k = len(cols)
+    types = (C.c_int32 * k)(*[NP_CODE[c.dtype] for c in cols])
+    ptrs = (C.c_void_p * k)(*[c.ctypes.data for c in cols])
+    nl = None
+    keep = []
+    if nulls is not None:
+        nw = [None if x is None else np.ascontiguousarray(x, dtype=np.uint64) for x in nulls]
+        keep = nw
+        nl = (C.c_void_p * k)(*[None if x is None else x.ctypes.data for x in nw])
+    desc = (C.c_int32 * k)(*[int(bool(d)) for d in (descending or [0] * k)])
+    out = np.empty(n, dtype=np.int32)
+    lib().oracle_order_by(k, types, ptrs, nl, desc, n, _p(out))
+    del keep
+    return out
 
 
 def indexes(mask: np.ndarray) -> np.ndarray:

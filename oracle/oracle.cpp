@@ -370,6 +370,57 @@ int64_t oracle_compact(int32_t elem_bytes, const void* in, const int8_t* mask, i
     return c;
 }
 
+// ORDER BY oracle (qikkDB/QueryEngine/GPUCore/GPUOrderBy.cuh:88-195 as the dispatcher drives it): the row
+// permutation that sorts by the columns, column 0 most significant, each ascending or descending, ties in input
+// order.  As the reference does, a NULL row takes the value lowest(T) before the comparison
+// (TransformNullValsToSmallestVal), and values compare the way its CUB radix sort orders them: integers by value,
+// IEEE values by their bits mapped to an unsigned order (negative: all bits flipped; else the sign bit set), so
+// -0.0 precedes +0.0.  Descending reverses the comparison only (the radix sort stays stable).
+namespace {
+uint64_t ob_key(int32_t type, const void* col, const uint64_t* nulls, int64_t r) {
+    const bool null = nulls && bit(nulls, r);
+    switch (type) {
+        case T_INT32: {
+            const int32_t v = null ? std::numeric_limits<int32_t>::lowest() : static_cast<const int32_t*>(col)[r];
+            return static_cast<uint32_t>(v) ^ 0x80000000u;
+        }
+        case T_INT64: {
+            const int64_t v = null ? std::numeric_limits<int64_t>::lowest() : static_cast<const int64_t*>(col)[r];
+            return static_cast<uint64_t>(v) ^ 0x8000000000000000ull;
+        }
+        case T_FLOAT: {
+            const float v = null ? std::numeric_limits<float>::lowest() : static_cast<const float*>(col)[r];
+            uint32_t b;
+            memcpy(&b, &v, 4);
+            return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+        }
+        default: {
+            const double v = null ? std::numeric_limits<double>::lowest() : static_cast<const double*>(col)[r];
+            uint64_t b;
+            memcpy(&b, &v, 8);
+            return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+        }
+    }
+}
+}  // namespace
+
+void oracle_order_by(int32_t n_cols, const int32_t* types, const void* const* cols, const uint64_t* const* nulls,
+                     const int32_t* descending, int64_t n, int32_t* out) {
+    std::vector<std::vector<uint64_t>> keys(n_cols, std::vector<uint64_t>(static_cast<size_t>(n)));
+    for (int c = 0; c < n_cols; ++c)
+        for (int64_t r = 0; r < n; ++r) keys[c][r] = ob_key(types[c], cols[c], nulls ? nulls[c] : nullptr, r);
+    std::vector<int32_t> idx(static_cast<size_t>(n));
+    for (int64_t r = 0; r < n; ++r) idx[r] = static_cast<int32_t>(r);
+    std::stable_sort(idx.begin(), idx.end(), [&](int32_t x, int32_t y) {
+        for (int c = 0; c < n_cols; ++c) {
+            const uint64_t a = keys[c][x], b = keys[c][y];
+            if (a != b) return (descending && descending[c]) ? a > b : a < b;
+        }
+        return false;
+    });
+    std::copy(idx.begin(), idx.end(), out);
+}
+
 int64_t oracle_indexes(const int8_t* mask, int64_t n, int32_t* out) {
     int64_t c = 0;
     for (int64_t i = 0; i < n; ++i)

@@ -157,6 +157,10 @@ SIGNATURES = [
     ("qdb_gb_batch_set_sharing", I32, [P, I32]),
     ("qdb_gb_batch_tuning_reset", I32, []),
     ("qdb_gb_plain_run", I32, [C.POINTER(qdb_gb_query), I32, I32, PI64, P]),
+    ("qdb_order_by_column", I32, [I32, P, P, I32, I64, I32, P, P]),
+    ("qdb_order_by", I32, [I32, P, P, P, P, I64, P, P]),
+    ("qdb_reorder", I32, [I32, P, P, I64, I64, P, P]),
+    ("qdb_reorder_nulls", I32, [P, P, I64, I64, P, P]),
     ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
     ("qdb_server_destroy", I32, [P]),
     ("qdb_server_submit", I32, [P, C.POINTER(qdb_gb_query), C.POINTER(C.c_uint64)]),

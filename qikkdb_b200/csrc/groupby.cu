@@ -378,10 +378,11 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
 
     // Spill plan: partitions small enough for the spill pass's table (one CTA per SM, the largest table shared
     // memory holds after the cell-fill prefix and the second-level counters) at half load.  The aggregation pass
-    // writes at most 2^kMaxSpillBits partitions (its (partition, CTA) cells then fit L2, which combines their partly
-    // written sectors); a table needing more has two levels: the spill pass over the first level aggregates what its
-    // table takes and sends the other rows to 2^spill_bits2 sub-partitions per partition, which a third pass
-    // aggregates.
+    // writes at most 2^kMaxSpillBits partitions; a table needing more has two levels: the spill pass over the first
+    // level aggregates what its table takes and sends the other rows to 2^spill_bits2 sub-partitions per partition,
+    // which a third pass aggregates.  (Measured on 2^27 rows over 16.8M groups: one level of 8192 partitions, whose
+    // 1.2M (partition, CTA) cells overflow L2 with partly written lines, still beats 1024 + 8 x 1024 partitions, whose
+    // extra pass over many small items costs more than the better-combined writes save.)
     int spill_bits = -1;
     int spill_bits2 = 0;
     int NB2 = 0;
@@ -395,9 +396,16 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
         NB2 = static_cast<int>(budget2 / bucket_bytes);
         if (NB2 >= 64 && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
             const uint64_t per = static_cast<uint64_t>(NB2);  // distinct keys per partition at half load
-            const uint64_t parts = next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per);
+            // At least four partitions per SM, so the spill pass's items balance over the SMs (the last wave of a
+            // pass with 1.7 items per SM leaves a quarter of them idle) ...
+            const uint64_t min_parts = next_pow2(4 * static_cast<uint64_t>(di.sm_count));
+            const uint64_t parts = std::max(min_parts, next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per));
             int bits = 0;
             while ((1ull << bits) < parts) ++bits;
+            // ... and a table sized for its partition's share of the groups at half load (the spill pass clears and
+            // scans every slot of it per item).
+            const uint64_t want = std::max<uint64_t>(64, next_pow2((static_cast<uint64_t>(gb->capacity) + parts - 1) / parts));
+            if (want < static_cast<uint64_t>(NB2)) NB2 = static_cast<int>(want);
             const int max1 = static_cast<int>(env_int("QDB_SPILL_BITS_MAX", kMaxSpillBits));
             if (bits <= max1) {
                 spill_bits = bits;

@@ -286,9 +286,7 @@ __device__ __forceinline__ uint64_t* g_find_from(const Region& R, int W, uint64_
     return nullptr;
 }
 
-// Home slot of a key whose mix64 hash is h: the top log2(cap) bits of h.  A key's spill partition (fast pass) is the
-// top bits of the same hash, so the groups of one partition live in one contiguous stretch of the table and the
-// spill pass's merge of a partition touches that stretch only.
+// Home slot of a key whose mix64 hash is h: the top log2(cap) bits of h (a multiply-high, no power-of-two mask).
 __device__ __forceinline__ uint64_t home_slot(const Region& R, uint64_t h) { return __umul64hi(h, R.mask + 1); }
 
 __device__ __forceinline__ uint64_t* g_find(const Region& R, int W, uint64_t key, uint64_t h,

@@ -35,7 +35,7 @@ constexpr int kFastR = 32 * kFastSeg;               // rows per warp and tile
 constexpr int kFastT = kFastWarps * kFastR;         // rows per tile (2048)
 constexpr int kDedupTrial = 4;                      // steps a warp runs with warp aggregation before deciding
 constexpr int kDedupGroup = 4;                      // lanes sharing a slot that are combined before the update
-constexpr int kMaxSpillBits = 10;                   // partitions the aggregation pass writes: at most 1024
+constexpr int kMaxSpillBits = 13;                   // partitions the aggregation pass writes: at most 8192
 constexpr int kMaxSpill2Bits = 6;                   // second-level partitions per first-level one: at most 64
 constexpr uint64_t kHashMul = 0x9E3779B97F4A7C15ull;
 
@@ -67,10 +67,10 @@ __device__ __forceinline__ FTab ftab(unsigned char* sm, const AggArgs& a) {
     return t;
 }
 
-// Hash of a key word for the shared tables: one 64-bit multiply (Fibonacci hashing, Knuth TAOCP vol. 3, 6.4).  Its
-// top 32 bits pick the bucket and bits 32..46 the bit of the seen-once filter.  The spill partition comes from the
-// independent mix64 hash (the global table's), so a partition's rows spread over every bucket of the spill pass's
-// table.
+// Hash of a key word for the shared tables and the spill: one 64-bit multiply (Fibonacci hashing, Knuth TAOCP vol. 3,
+// 6.4).  Its top bits pick the spill partition, the 32 bits below bit `shift` (32 - partition bits) the bucket (so
+// a partition's rows spread over every bucket of the spill pass's table), and bits 32..46 the bit of the seen-once
+// filter.  The global table hashes with the independent mix64.
 __device__ __forceinline__ uint64_t fhash(uint64_t kw) { return kw * kHashMul; }
 __device__ __forceinline__ uint32_t fbucket(uint64_t m, int shift, uint32_t NB) {
     const uint32_t x = __funnelshift_rc(static_cast<uint32_t>(m), static_cast<uint32_t>(m >> 32), shift);
@@ -318,7 +318,7 @@ struct FastWarp {
     int trial = 0;         // steps run so far in the warp-aggregation trial
     unsigned trial_hits = 0, trial_leaders = 0;  // warp totals over the trial
     unsigned hits = 0, tries = 0;
-    // Where a miss goes: partition q = (mix64(key) >> part_shift) & part_mask, appended to cell cell_base + q cell_mul
+    // Where a miss goes: partition q = (fhash(key) >> part_shift) & part_mask, appended to cell cell_base + q cell_mul
     // of spill_out (records of 16 bytes, or 8 for a count-only table) at the position its shared fill counter
     // sfill[q] hands out; a full cell sends the row to the global table.
     uint32_t sfill = 0;    // shared-window address of the per-partition fill counters
@@ -422,26 +422,17 @@ struct FastWarp {
         if (hit && !big) update(static_cast<uint32_t>(slot), 1u, q, e, e);
     }
 
-    // A row the shared table did not take: appended to its partition's spill cell, or inserted into the global table.
-    __device__ __forceinline__ void miss_row(uint64_t kw, VT v, bool spillable) {
-        if (spill_ok && spillable) {
-            // The partition comes from the key's mix64 hash, whose top bits are its home slot in the global table.
-            const uint32_t p = part_shift < 64 ? static_cast<uint32_t>(mix64(kw) >> part_shift) & part_mask : 0u;
-            const unsigned pos = atoms_add(sfill + p * 4u, 1u);
-            if (pos < cell_cap) {
-                // One record per row (key word, value bits): a single 8- or 16-byte store.
-                const uint64_t idx = static_cast<uint64_t>(cell_base + static_cast<int64_t>(p) * cell_mul) * cell_cap + pos;
-                if constexpr (VALS) {
-                    uint64_t vb = 0;
-                    memcpy(&vb, &v, sizeof(VT));
-                    reinterpret_cast<ulonglong2*>(spill_out)[idx] = make_ulonglong2(kw, vb);
-                } else {
-                    spill_out[idx] = kw;
-                }
-                return;
-            }
+    // Stores a spilled row as one record (key word, value bits: a single 8- or 16-byte store) at position pos of its
+    // partition's cell.
+    __device__ __forceinline__ void spill_store(uint64_t kw, VT v, uint32_t p, unsigned pos) {
+        const uint64_t idx = static_cast<uint64_t>(cell_base + static_cast<int64_t>(p) * cell_mul) * cell_cap + pos;
+        if constexpr (VALS) {
+            uint64_t vb = 0;
+            memcpy(&vb, &v, sizeof(VT));
+            reinterpret_cast<ulonglong2*>(spill_out)[idx] = make_ulonglong2(kw, vb);
+        } else {
+            spill_out[idx] = kw;
         }
-        global_row(kw, v);
     }
 
     // Two rows per lane: (act[u], kw[u], v[u]) for u = 0, 1.  The two rows' loads and arithmetic are independent, so
@@ -541,9 +532,26 @@ struct FastWarp {
 #pragma unroll
         for (int u = 0; u < 2; ++u) miss[u] = act[u] & !hit[u];
         if (__any_sync(0xffffffffu, miss[0] | miss[1])) {
+            // Both rows' spill positions are claimed before either record is stored, so the two shared-atomic round
+            // trips overlap; rows that cannot spill (or whose cell is full) go to the global table.
+            bool sp[2];
+            unsigned pos[2];
+            uint32_t part[2];
 #pragma unroll
-            for (int u = 0; u < 2; ++u)
-                if (miss[u]) miss_row(kw[u], v[u], (kw[u] != kEmpty) & inwin[u]);
+            for (int u = 0; u < 2; ++u) {
+                sp[u] = miss[u] & spill_ok & (kw[u] != kEmpty) & inwin[u];
+                part[u] = (sp[u] && part_shift < 64) ? static_cast<uint32_t>(m[u] >> part_shift) & part_mask : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) pos[u] = sp[u] ? atoms_add(sfill + part[u] * 4u, 1u) : 0u;
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (sp[u] && pos[u] < cell_cap) {
+                    spill_store(kw[u], v[u], part[u], pos[u]);
+                } else if (miss[u]) {
+                    global_row(kw[u], v[u]);
+                }
+            }
         }
     }
 };
@@ -959,7 +967,7 @@ __global__ void __launch_bounds__(kFSpillThreads, 1) gb_fspill_kernel(const AggA
         const int hb = max(1, 64 - __clzll(static_cast<long long>(total)));
         const FixQ fq = fixq<VT>(s_emax == INT_MIN ? 0 : s_emax, hb);
         FastWarp<VT, MODE> fw(a, tab, fq, &s_claims);
-        fw.bshift = 32;
+        fw.bshift = 32 - a.spill_bits;
         fw.fits = a.fits != 0;
         fw.probe_b = a.probe_b;
         fw.dedup = a.dedup != 0;

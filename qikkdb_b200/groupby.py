@@ -433,3 +433,54 @@ class GPUReconstruct:
         capi.check(capi.lib().qdb_compress_null_mask(_ptr(inArray), int(dataElementCount), C.byref(out),
                                                      _stream(stream)))
         return DeviceBuffer(out.value, nullmask_words(dataElementCount), np.uint64)
+
+
+class GPUOrderBy:
+    """GPUOrderBy (qikkDB/QueryEngine/GPUCore/GPUOrderBy.cuh:88-195): the dispatcher calls OrderByColumn for the
+    ORDER BY columns from the last to the first, then reorders every result column by the indices
+    (ReOrderByIdx / ReOrderNullValuesByIdx).  NULL rows order as lowest(T); ties keep their input order."""
+
+    ASC = 0   # OrderBy::Order::ASC
+    DESC = 1  # OrderBy::Order::DESC
+
+    def __init__(self, dataElementCount: int, stream=None):
+        self.n = int(dataElementCount)
+        self.indices = torch.empty(max(self.n, 1), dtype=torch.int32, device="cuda")
+        self.first = True
+        self.stream = stream
+
+    def OrderByColumn(self, outIndices: Optional[torch.Tensor], inCol: torch.Tensor, nullBitMask,
+                      dataElementCount: int, order: int) -> None:
+        capi.check(capi.lib().qdb_order_by_column(type_code(inCol.dtype), _ptr(inCol), _ptr(nullBitMask), int(order),
+                                                  int(dataElementCount), 1 if self.first else 0, _ptr(self.indices),
+                                                  _stream(self.stream)))
+        self.first = False
+        if outIndices is not None and dataElementCount:
+            outIndices[:dataElementCount].copy_(self.indices[:dataElementCount])
+
+    @staticmethod
+    def ReOrderByIdx(outCol: torch.Tensor, inIndices: torch.Tensor, inCol: torch.Tensor, dataElementCount: int,
+                     offset: int = 0, stream=None) -> None:
+        """outCol[i] = inCol[inIndices[offset + i]] for i < dataElementCount (OFFSET / LIMIT)."""
+        capi.check(capi.lib().qdb_reorder(inCol.element_size(), _ptr(inCol), _ptr(inIndices), int(offset),
+                                          int(dataElementCount), _ptr(outCol), _stream(stream)))
+
+    @staticmethod
+    def ReOrderNullValuesByIdx(outNullBitMask: torch.Tensor, indices: torch.Tensor, inNullBitMask: torch.Tensor,
+                               rowCount: int, offset: int = 0, stream=None) -> None:
+        capi.check(capi.lib().qdb_reorder_nulls(_ptr(inNullBitMask), _ptr(indices), int(offset), int(rowCount),
+                                                _ptr(outNullBitMask), _stream(stream)))
+
+
+def order_by(cols: Sequence[torch.Tensor], descending: Optional[Sequence[bool]] = None, nulls=None,
+             stream=None) -> torch.Tensor:
+    """Row permutation of ORDER BY cols[0], cols[1], ... (qdb_order_by): int32 device tensor."""
+    n = cols[0].numel()
+    out = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    k = len(cols)
+    types = (C.c_int32 * k)(*[type_code(c.dtype) for c in cols])
+    ptrs = (C.c_void_p * k)(*[_ptr(c) for c in cols])
+    nl = (C.c_void_p * k)(*[_ptr(x) for x in nulls]) if nulls is not None else None
+    desc = (C.c_int32 * k)(*[int(bool(d)) for d in (descending or [False] * k)])
+    capi.check(capi.lib().qdb_order_by(k, types, ptrs, nl, desc, n, _ptr(out), _stream(stream)))
+    return out[:n]

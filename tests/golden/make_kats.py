@@ -184,6 +184,19 @@ cases.append({
     "expected_groups": unique, "expected_value_all": 7,
 })
 
+# GROUP BY + ORDER BY (DispatcherGroupByTests.cpp:1551-1588): SELECT colInteger, SUM(colID) ... GROUP BY colInteger
+# ORDER BY colInteger (resp. ORDER BY SUM(colID) - 2, the same order as SUM(colID)), colID the row number; the
+# expected rows in the order the tests assert.
+order_cases = []
+OBK = [10, 10, 2, 2, 6, 6, 4, 4, 8, 8]
+order_cases.append({"name": "IntegerSimpleSumOrderByKeys", "source": DGB + ":1551", "agg": "sum", "keys": OBK,
+                    "values": list(range(len(OBK))), "order_by": "key", "descending": False,
+                    "expected": [[2, 5], [4, 13], [6, 9], [8, 17], [10, 1]]})
+order_cases.append({"name": "IntegerSimpleSumOrderByValues", "source": DGB + ":1569", "agg": "sum", "keys": OBK,
+                    "values": list(range(len(OBK))), "order_by": "value", "descending": False,
+                    "expected": [[10, 1], [2, 5], [6, 9], [4, 13], [8, 17]]})
+
 with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
-    json.dump({"generated_by": "tests/golden/make_kats.py", "cases": cases}, f, indent=1)
-print(len(cases), "cases")
+    json.dump({"generated_by": "tests/golden/make_kats.py", "cases": cases, "order_by_cases": order_cases}, f,
+              indent=1)
+print(len(cases), "cases,", len(order_cases), "ORDER BY cases")

@@ -33,7 +33,8 @@ def test_filtered_zipf_256m(cuda):
 
 
 def test_composite_128m(cuda):
-    """(int32, int32) keys uniform over 4096 x 4096, int64 values in [0, 2^31); SUM/COUNT/MAX bit for bit."""
+    """(int32, int32) keys uniform over 4096 x 4096, int64 values in [0, 2^31); SUM/COUNT/MAX bit for bit.  8192 spill
+    partitions in one level."""
     n = 1 << 27
     a = dg.uniform_i32(42, 0, n, 0, 4095)
     b = dg.uniform_i32(42, 1, n, 0, 4095)

@@ -11,40 +11,46 @@ from test_gpu_parity import run_both
 
 pytestmark = pytest.mark.gpu
 
-# The aggregation pass picks a row's spill partition, and the global table its home slot, from the top bits of the
-# key's mix64 hash: h = x ^ x >> 33, x * M1, ^ >> 33, * M2, ^ >> 33 (every step invertible modulo 2^64).
-MIX_M1 = 0xFF51AFD7ED558CCD
-MIX_M2 = 0xC4CEB9FE1A85EC53
-MASK64 = (1 << 64) - 1
-
-
-def mix64_inverse(h: int) -> int:
-    x = h ^ (h >> 33)
-    x = (x * pow(MIX_M2, -1, 1 << 64)) & MASK64
-    x ^= x >> 33
-    x = (x * pow(MIX_M1, -1, 1 << 64)) & MASK64
-    return x ^ (x >> 33)
+# The aggregation pass picks a row's spill partition from the top bits of key * C (mod 2^64); the global table hashes
+# keys with the independent mix64.
+SPILL_HASH = 0x9E3779B97F4A7C15
 
 
 def keys_in_partition_zero(count: int, seed: int) -> np.ndarray:
-    """Distinct int64 keys whose spill partition is 0 for every partition count up to 2^13: k = mix64^-1(t) with
-    t < 2^51, so the top 13 bits of the key's hash are zero (and the keys' home slots crowd the table's first
-    stretch)."""
+    """Distinct int64 keys whose spill partition is 0 for every partition count up to 2^14 (first and second level
+    together): k = t * C^-1 mod 2^64 with t < 2^50, so the top 14 bits of k * C are zero."""
+    inv = pow(SPILL_HASH, -1, 1 << 64)
     rng = np.random.default_rng(seed)
-    t = np.unique(rng.integers(1, 1 << 51, count + count // 8, dtype=np.uint64))[:count]
-    k = np.array([mix64_inverse(int(x)) for x in t], dtype=np.uint64).astype(np.int64)
+    t = np.unique(rng.integers(1, 1 << 50, count + count // 8, dtype=np.uint64))[:count]
+    k = (t * np.uint64(inv)).astype(np.int64)  # wraps modulo 2^64
     assert len(np.unique(k)) == count
     return k
 
 
-def test_spill_cells_overflow_to_global(cuda, monkeypatch):
+def test_spill_cells_overflow_to_global_default_tables(cuda):
+    """200000 keys in spill partition 0 with the default table sizes: the CTAs' cells of that partition overflow and
+    the spill pass's table cannot hold the partition, so rows take the global-table path on both sides."""
+    n = 1 << 21
+    uniq = keys_in_partition_zero(200_000, 5)
+    pick = dg.uniform_i32(51, 0, n, 0, len(uniq) - 1)
+    k = uniq[pick]
+    v = dg.lognormal_f32(51, 1, n, 2.0, 1.0)
+    p = dg.uniform_f32(51, 2, n)
+    rel, g, _ = run_both(k, v, ["sum", "avg", "count", "min", "max"], 1 << 20, 0,
+                         pred=(p, FilterConditions.less, 0.7, np.float32, None), val_is_float=True)
+    assert rel <= FLOAT_RTOL and g["n_groups"] > 100_000
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_spill_cells_overflow_to_global(cuda, monkeypatch, levels):
     """Every key lands in spill partition 0.  With both shared tables cut down (64 buckets in the aggregation pass,
-    8 KB in the spill pass, hence 8192 partitions), the CTAs' cells of that partition overflow and the spill pass's
-    table cannot hold the partition, so rows take the global-table path on both sides.  (The same keys crowd the
-    start of the global table, whose home slots share the partition's hash bits: 3000 of them keep the probe runs
-    short.)"""
+    8 KB in the spill pass, hence 8192 partitions, written in one level or, with at most 1024 partitions per pass, in
+    two), the CTAs' cells of that partition overflow and the spill pass's table cannot hold the partition, so rows
+    take the global-table path on every side."""
     monkeypatch.setenv("QDB_FAST_BUCKETS", "64")
     monkeypatch.setenv("QDB_SPILL_SMEM_KB", "8")
+    if levels == 2:
+        monkeypatch.setenv("QDB_SPILL_BITS_MAX", "10")
     n = 1 << 19
     uniq = keys_in_partition_zero(3000, 5)
     pick = dg.uniform_i32(51, 0, n, 0, len(uniq) - 1)
@@ -127,3 +133,14 @@ def test_tables_on_two_streams_share_the_spill_area(cuda):
     for t, (k, v) in zip(tables, cols):
         rel = compare(t.results_numpy(), oracle.groupby(k, v), ["sum", "count", "max"], True)
         assert rel <= FLOAT_RTOL
+
+
+def test_two_level_spill_composite(cuda, monkeypatch):
+    """A composite-key table whose groups need 4096 spill partitions, written as 1024 first-level partitions of 4
+    sub-partitions each (the two-level spill): SUM/COUNT/MAX bit for bit."""
+    monkeypatch.setenv("QDB_SPILL_BITS_MAX", "10")
+    n = 1 << 23
+    a = dg.uniform_i32(32, 0, n, 0, 4095)
+    b = dg.uniform_i32(32, 1, n, 0, 4095)
+    v = dg.uniform_i64(32, 2, n, 0, (1 << 31) - 1)
+    run_both([a, b], v, ["sum", "count", "max"], 1 << 23)
