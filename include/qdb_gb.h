@@ -261,6 +261,53 @@ int32_t qdb_reorder(int32_t elem_bytes, const void* in, const int32_t* indices, 
 int32_t qdb_reorder_nulls(const uint64_t* in, const int32_t* indices, int64_t offset, int64_t count, uint64_t* out,
                           void* stream);
 
+/* ---- scalar aggregation: GPUAggregation::col<AGG, OUT, IN> (qikkDB/QueryEngine/GPUCore/GPUAggregation.cuh:15-37)
+ * over a WHERE-filtered column, fused, accumulated over a query's blocks ----
+ * A qdb_scalar accumulates COUNT, SUM, MIN and MAX of one value column (val_type INT32, INT64, FLOAT or DOUBLE) over
+ * every qdb_scalar_process call: rows that pass `pred` (optional, `col OP constant` as in qdb_gb_process) and `mask`
+ * (optional int8, non-zero = keep) and whose value is not NULL (val_nulls optional).  qdb_scalar_result reads one
+ * aggregate (one qdb_agg bit) into *out_value, typed as the GROUP BY results are: V for MIN/MAX/SUM/AVG (an integer
+ * SUM wraps in V, an integer AVG is the wrapped sum over the count, truncated; float sums are accumulated in FP64),
+ * int64 for COUNT; *out_is_null is 1 for MIN/MAX/SUM/AVG over no row.  qdb_scalar_result synchronises `stream`. */
+typedef struct qdb_scalar qdb_scalar; /* opaque scalar accumulator */
+int32_t qdb_scalar_create(qdb_scalar** out, int32_t val_type, void* stream);
+int32_t qdb_scalar_destroy(qdb_scalar* q);
+int32_t qdb_scalar_reset(qdb_scalar* q, void* stream);
+int32_t qdb_scalar_process(qdb_scalar* q, const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
+                           const int8_t* mask, void* stream);
+int32_t qdb_scalar_result(qdb_scalar* q, int32_t agg, void* out_value, int32_t* out_is_null, void* stream);
+/* Block skipping (GpuSqlDispatcher::WhereEvaluation, qikkDB/GpuSqlParser/GpuSqlDispatcher.cpp:1116-1125): whether a
+ * block whose predicate column has non-NULL values in [*block_min, *block_max] (host values of pred->type) can hold a
+ * row passing `pred`; *may_pass = 0 lets the caller skip loading and processing the block.  Host only. */
+int32_t qdb_pred_block_may_pass(const qdb_pred* pred, const void* block_min, const void* block_max, int32_t* may_pass);
+
+/* ---- GROUP BY over string keys: GPUGroupBy<AGG, O, std::string, V>
+ *      (qikkDB/QueryEngine/GPUCore/GPUGroupByString.cuh:171-785, kernel :39-169) ----
+ * Keys come in the reference's GPUString layout (GPUMemory.cuh GPUString): `chars` all characters concatenated,
+ * `ends[i]` the int64 end offset of string i (string i is chars[i ? ends[i-1] : 0, ends[i])).  qdb_gbs_create sizes
+ * the table for max_groups distinct non-NULL keys (the NULL key has its own slot, as keyBufferSize_ adds one) and a
+ * key arena of max_key_bytes characters (<= 0: 32 per group).  agg_mask as qdb_gb_create; val_type 0 is allowed with
+ * QDB_AGG_COUNT only and counts rows.  qdb_gbs_process (asynchronous) aggregates the rows whose `mask` (optional
+ * int8, non-zero = keep) is set (a COUNT-only table given no `vals` counts rows); NULL keys (key_nulls, optional)
+ * form one group; NULL values (val_nulls, optional)
+ * are skipped, a group whose values are all NULL has a NULL aggregate and COUNT 0.  More distinct keys than
+ * max_groups, or more key characters than the arena holds, latch QDB_HASH_TABLE_FULL, which qdb_gbs_check (it
+ * synchronises `stream`) returns and clears.  qdb_gbs_results (GetResults, GPUGroupByString.cuh:446-563) allocates
+ * the result keys as a GPUString (*out_chars, *out_ends), their NULL bitmask (optional), and per requested aggregate
+ * (aggs[n_aggs], n_aggs <= 5) a column typed as qdb_gb_results types it plus its NULL bitmask (optional array);
+ * an empty result yields NULL pointers and count 0.  It synchronises `stream`. */
+typedef struct qdb_gbs qdb_gbs; /* opaque string-key GROUP BY table */
+int32_t qdb_gbs_create(qdb_gbs** out, int32_t agg_mask, int32_t val_type, int64_t max_groups, int64_t max_key_bytes,
+                       void* stream);
+int32_t qdb_gbs_destroy(qdb_gbs* g);
+int32_t qdb_gbs_reset(qdb_gbs* g, void* stream);
+int32_t qdb_gbs_process(qdb_gbs* g, const char* chars, const int64_t* ends, const uint64_t* key_nulls, const void* vals,
+                        const uint64_t* val_nulls, const int8_t* mask, int64_t n, void* stream);
+int32_t qdb_gbs_check(qdb_gbs* g, void* stream);
+int32_t qdb_gbs_results(qdb_gbs* g, int32_t n_aggs, const int32_t* aggs, char** out_chars, int64_t** out_ends,
+                        uint64_t** out_key_nulls, void** out_vals, uint64_t** out_val_nulls, int64_t* out_count,
+                        void* stream);
+
 /* ---- batched GROUP BY: many independent queries in one persistent launch ----
  * The reference runs one GPUGroupBy per query, each with its own kernel launches and host synchronisations
  * (GpuSqlDispatcherAggregationFunctions.h:377-507 via GroupByHelper, :99-318).  A batch holds up to

@@ -6,10 +6,12 @@
  * GPUMemory::free) and error behaviour (a query_engine_error carrying the QueryEngineErrorType) are those of
  *   GPUGroupBy<AGG,O,K,V>                 qikkDB/QueryEngine/GPUCore/GPUGroupBy.cuh:285-790
  *   GPUGroupBy<AGG,O,std::vector<void*>,V> qikkDB/QueryEngine/GPUCore/GPUGroupByMultiKey.cuh:262-912
+ *   GPUGroupBy<AGG,O,std::string,V>       qikkDB/QueryEngine/GPUCore/GPUGroupByString.cuh:171-785
  *   GPUBinary<FilterConditions::OP,int8_t,L,R>::Binary   GPUBinary.cuh:555-579
  *   GPUReconstruct::{reconstructColKeep, reconstructCol, GenerateIndexesKeep, GenerateIndexes, PrefixSum,
  *                    CompressNullMask}   GPUReconstruct.cuh:204-640
  *   GPUOrderBy::{OrderByColumn, ReOrderByIdx, ReOrderNullValuesByIdx}   GPUOrderBy.cuh:88-195
+ *   GPUAggregation::col<AGG, OUT, IN>      GPUAggregation.cuh:15-37
  *   GPUMemory::{alloc, allocAndSet, free, copyHostToDevice, copyDeviceToHost, copyDeviceToDevice, memset}
  *                                          GPUMemory.cuh:18-236
  *   query_engine_error / gpu_error / QueryEngineErrorType   qikkDB/QueryEngine/GPUError.h:17-75
@@ -177,6 +179,16 @@ inline void copyDeviceToDevice(T* dst, const T* src, size_t dataElementCount) {
 }
 /* Words of a null bitmask for dataElementCount rows (NullValues.cu:13-16). */
 inline size_t CalculateNullMaskSize(size_t dataElementCount) { return (dataElementCount + 63) / 64; }
+/* A device string column (GPUMemory.cuh GPUString): every string's characters concatenated, and the int64 end
+ * offset of each string (string i is allChars[i ? stringIndices[i-1] : 0, stringIndices[i])). */
+struct GPUString {
+    char* allChars;
+    int64_t* stringIndices;
+};
+inline void free(GPUString s) {
+    free(s.allChars);
+    free(s.stringIndices);
+}
 }  // namespace GPUMemory
 
 /* Owning device pointer (cuda_ptr.h): freed with GPUMemory::free. */
@@ -523,6 +535,64 @@ private:
     qdb_cpp::table t_;
 };
 
+/* ---- GPUGroupBy<AGG, O, std::string, V>: GROUP BY over string keys (GPUGroupByString.cuh:171-785) ----
+ * The keys arrive as a GPUString block.  The table keeps its own copy of every distinct key (a device arena of
+ * 32 characters per group on average); GetResults returns the keys as a newly allocated GPUString (release it
+ * with GPUMemory::free).  COUNT given no values (inValues NULL) counts rows. */
+template <typename AGG, typename O, typename V>
+class GPUGroupBy<AGG, O, std::string, V> : public IGroupBy {
+    static_assert(qdb_cpp::output_type_ok<AGG, O, V>(),
+                  "GROUP BY output type: O must be int64_t for COUNT and V for MIN, MAX, SUM and AVG");
+
+public:
+    /* GPUGroupBy(maxHashCount, keySizeMultiplier) (GPUGroupByString.cuh:210): up to
+     * min(maxHashCount * keySizeMultiplier, 2^30) distinct non-NULL keys, plus the NULL key. */
+    GPUGroupBy(const int32_t maxHashCount, const int32_t keySizeMultiplier)
+        : max_groups_(qdb_cpp::table_size(maxHashCount, keySizeMultiplier)) {
+        qdb_cpp::check(qdb_gbs_create(&g_, AGG::bit, AGG::bit ? qdb_cpp::type_of<V>::code : 0, max_groups_, 0, nullptr));
+    }
+    ~GPUGroupBy() {
+        if (g_) qdb_gbs_destroy(g_);
+    }
+    GPUGroupBy(const GPUGroupBy&) = delete;
+    GPUGroupBy& operator=(const GPUGroupBy&) = delete;
+
+    /* ProcessBlock (GPUGroupByString.cuh:333): throws query_engine_error(GPU_HASH_TABLE_FULL) when the block
+     * brings more distinct keys than the table holds. */
+    void ProcessBlock(GPUMemory::GPUString inKeys, V* inValues, int32_t dataElementCount,
+                      nullmask_t* inKeysNullMask = nullptr, nullmask_t* inValuesNullMask = nullptr) {
+        if (dataElementCount <= 0) return;
+        qdb_cpp::check(qdb_gbs_process(g_, inKeys.allChars, inKeys.stringIndices, inKeysNullMask,
+                                       AGG::bit ? inValues : nullptr, AGG::bit ? inValuesNullMask : nullptr, nullptr,
+                                       dataElementCount, nullptr));
+        qdb_cpp::check(qdb_gbs_check(g_, nullptr));
+    }
+
+    /* GetMaxHashCount: the key buffer size, max_groups plus the NULL slot. */
+    int32_t GetMaxHashCount() { return static_cast<int32_t>(max_groups_ + 1); }
+
+    /* GetResults (GPUGroupByString.cuh:446): newly allocated keys and values (NULL pointers and a count of 0 for
+     * an empty result).  outValues stays NULL for AGG none. */
+    void GetResults(GPUMemory::GPUString* outKeys, O** outValues, int32_t* outDataElementCount,
+                    nullmask_t** outKeysNullMask = nullptr, nullmask_t** outValuesNullMask = nullptr) {
+        const int32_t agg = AGG::bit;
+        void* v = nullptr;
+        uint64_t* vn = nullptr;
+        int64_t count = 0;
+        qdb_cpp::check(qdb_gbs_results(g_, agg ? 1 : 0, &agg, &outKeys->allChars, &outKeys->stringIndices,
+                                       reinterpret_cast<uint64_t**>(outKeysNullMask), agg ? &v : nullptr,
+                                       agg && outValuesNullMask ? &vn : nullptr, &count, nullptr));
+        *outDataElementCount = static_cast<int32_t>(count);
+        if (outValues) *outValues = static_cast<O*>(v);
+        else GPUMemory::free(v);
+        if (outValuesNullMask) *outValuesNullMask = reinterpret_cast<nullmask_t*>(vn);
+    }
+
+private:
+    qdb_gbs* g_ = nullptr;
+    int64_t max_groups_;
+};
+
 /* Releases the key columns returned by the multi-key GetResults (GPUGroupByMultiKey.cu:403-418). */
 inline void FreeKeysVector(std::vector<void*> keysVector, std::vector<DataType> keyTypes) {
     for (size_t i = 0; i < keysVector.size() && i < keyTypes.size(); ++i) GPUMemory::free(keysVector[i]);
@@ -635,6 +705,27 @@ public:
         qdb_cpp::check(qdb_compress_null_mask(inputNullArray, dataElementCount, &out, nullptr));
         qdb_cpp::sync();
         return cuda_ptr<nullmask_t>(reinterpret_cast<nullmask_t*>(out));
+    }
+};
+
+/* ---- GPUAggregation::col<AGG, OUT, IN> (GPUAggregation.cuh:15-37): one aggregate of a whole device column into
+ * the device value *outValue.  OUT is IN for MIN/MAX/SUM/AVG (an integer SUM wraps in IN, an integer AVG truncates)
+ * and int64_t for COUNT; an empty column leaves 0. ---- */
+class GPUAggregation {
+public:
+    template <typename AGG, typename OUT, typename IN>
+    static void col(OUT* outValue, IN* ACol, int32_t dataElementCount) {
+        static_assert(qdb_cpp::output_type_ok<AGG, OUT, IN>(), "aggregate output type: OUT = IN, or int64_t for COUNT");
+        static_assert(!std::is_same<AGG, AggregationFunctions::none>::value, "GPUAggregation needs an aggregate");
+        qdb_scalar* q = nullptr;
+        qdb_cpp::check(qdb_scalar_create(&q, qdb_cpp::type_of<IN>::code, nullptr));
+        OUT v{};
+        int32_t is_null = 0;
+        int32_t rc = qdb_scalar_process(q, ACol, nullptr, dataElementCount, nullptr, nullptr, nullptr);
+        if (rc == QDB_OK) rc = qdb_scalar_result(q, AGG::bit, &v, &is_null, nullptr);
+        qdb_scalar_destroy(q);
+        qdb_cpp::check(rc);
+        GPUMemory::copyHostToDevice(outValue, &v, 1);
     }
 };
 

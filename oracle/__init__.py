@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
         L.oracle_prefix_sum.argtypes = [P, I64, P]
         L.oracle_reference_filter_inputs.argtypes = [I32, I32, I64, P, P]
         L.oracle_order_by.argtypes = [I32, P, P, P, P, I64, P]
+        L.oracle_string_ids.restype = I64
+        L.oracle_string_ids.argtypes = [P, P, P, I64, P]
         _lib = L
     return _lib
 
@@ -113,6 +115,37 @@ def groupby(keys, vals=None, key_nulls=None, val_nulls=None, pred=None, mask=Non
         return out
     finally:
         L.oracle_result_free(r)
+
+
+def pack_strings(strings) -> tuple[np.ndarray, np.ndarray]:
+    """GPUString layout of a list of str/bytes (None counts as an empty string): (uint8 chars, int64 end offsets)."""
+    bs = [b"" if s is None else (s.encode() if isinstance(s, str) else bytes(s)) for s in strings]
+    lens = np.fromiter((len(b) for b in bs), dtype=np.int64, count=len(bs))
+    ends = np.cumsum(lens, dtype=np.int64)
+    chars = np.frombuffer(b"".join(bs), dtype=np.uint8).copy() if bs else np.zeros(0, dtype=np.uint8)
+    return chars, ends
+
+
+def string_at(chars: np.ndarray, ends: np.ndarray, i: int) -> bytes:
+    b = int(ends[i - 1]) if i else 0
+    return chars[b:int(ends[i])].tobytes()
+
+
+def groupby_string(chars, ends, vals=None, key_nulls=None, val_nulls=None, mask=None, threads: int = 0) -> dict:
+    """CPU GROUP BY over string keys: every string maps to the row of its first occurrence, then the integer GROUP BY
+    runs over those ids.  Returns {key (bytes, or None for the NULL key): {cnt, sum, min, max, avg, val_null}}."""
+    chars = np.ascontiguousarray(chars, dtype=np.uint8)
+    ends = np.ascontiguousarray(ends, dtype=np.int64)
+    n = len(ends)
+    ids = np.empty(n, dtype=np.int64)
+    kn = None if key_nulls is None else np.ascontiguousarray(key_nulls, dtype=np.uint64)
+    lib().oracle_string_ids(_p(chars) if len(chars) else None, _p(ends), _p(kn), n, _p(ids))
+    r = groupby(ids, vals, key_nulls=kn, val_nulls=val_nulls, mask=mask, threads=threads)
+    out = {}
+    for j in range(r["count"]):
+        key = None if r["key_nulls"][0][j] else string_at(chars, ends, int(r["keys"][0][j]))
+        out[key] = {f: r[f][j] for f in ("cnt", "sum", "min", "max", "avg", "val_null")}
+    return out
 
 
 def filter_mask(op: int, a, b, nulls=None, n: int | None = None) -> np.ndarray:

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <limits>
 #include <random>
+#include <string_view>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -419,6 +420,25 @@ void oracle_order_by(int32_t n_cols, const int32_t* types, const void* const* co
         return false;
     });
     std::copy(idx.begin(), idx.end(), out);
+}
+
+// String keys (GPUString layout: concatenated chars, int64 end offsets).  The reference's string GROUP BY
+// identifies a group by the row of the key's first occurrence (sourceIndices, GPUGroupByString.cuh:39-169);
+// this writes that row for every non-NULL row (rows with a NULL key get -1), so that GROUP BY over strings is
+// the integer GROUP BY above over these ids.  Returns the number of distinct non-NULL strings.
+int64_t oracle_string_ids(const char* chars, const int64_t* ends, const uint64_t* knull, int64_t n, int64_t* out) {
+    std::unordered_map<std::string_view, int64_t> first;
+    first.reserve(static_cast<size_t>(n < 1024 ? 1024 : n / 4));
+    for (int64_t i = 0; i < n; ++i) {
+        if (bit(knull, i)) {
+            out[i] = -1;
+            continue;
+        }
+        const int64_t b = i ? ends[i - 1] : 0;
+        const std::string_view s(chars + b, static_cast<size_t>(ends[i] - b));
+        out[i] = first.emplace(s, i).first->second;
+    }
+    return static_cast<int64_t>(first.size());
 }
 
 int64_t oracle_indexes(const int8_t* mask, int64_t n, int32_t* out) {

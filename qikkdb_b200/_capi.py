@@ -161,6 +161,18 @@ SIGNATURES = [
     ("qdb_order_by", I32, [I32, P, P, P, P, I64, P, P]),
     ("qdb_reorder", I32, [I32, P, P, I64, I64, P, P]),
     ("qdb_reorder_nulls", I32, [P, P, I64, I64, P, P]),
+    ("qdb_scalar_create", I32, [PP, I32, P]),
+    ("qdb_scalar_destroy", I32, [P]),
+    ("qdb_scalar_reset", I32, [P, P]),
+    ("qdb_scalar_process", I32, [P, P, P, I64, C.POINTER(qdb_pred), P, P]),
+    ("qdb_scalar_result", I32, [P, I32, P, C.POINTER(I32), P]),
+    ("qdb_gbs_create", I32, [PP, I32, I32, I64, I64, P]),
+    ("qdb_gbs_destroy", I32, [P]),
+    ("qdb_gbs_reset", I32, [P, P]),
+    ("qdb_gbs_process", I32, [P, P, P, P, P, P, P, I64, P]),
+    ("qdb_gbs_check", I32, [P, P]),
+    ("qdb_gbs_results", I32, [P, I32, P, PP, PP, PP, PP, PP, C.POINTER(I64), P]),
+    ("qdb_pred_block_may_pass", I32, [C.POINTER(qdb_pred), P, P, C.POINTER(I32)]),
     ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
     ("qdb_server_destroy", I32, [P]),
     ("qdb_server_submit", I32, [P, C.POINTER(qdb_gb_query), C.POINTER(C.c_uint64)]),

@@ -326,6 +326,14 @@ class GPUGroupBy:
         if agg in ("min", "max", "sum") and np.dtype(O) != np.dtype(V):
             raise QueryEngineError(GPU_EXTENSION_ERROR, "Input and output value data type must be the same in GROUP BY")
         self.agg = agg
+        self.string_keys = K is str
+        if self.string_keys:
+            # GPUGroupBy<AGG, O, std::string, V> (qikkDB/QueryEngine/GPUCore/GPUGroupByString.cuh:171-785)
+            self.n_key_cols = 1
+            self.max_groups = min(int(maxHashCount) * int(keySizeMultiplier), 1 << 30)
+            self.table = StringGroupByTable([agg] if agg != "none" else [], V if agg != "none" else None,
+                                            self.max_groups)
+            return
         multi = isinstance(K, (list, tuple))
         if multi and (len(K) != 2 or any(k != COLUMN_INT for k in K)):
             raise QueryEngineError(GPU_EXTENSION_ERROR, "multi-key GROUP BY supports (COLUMN_INT, COLUMN_INT) keys")
@@ -342,6 +350,8 @@ class GPUGroupBy:
                            inValuesNullMask if self.agg != "none" else None)
 
     def GetMaxHashCount(self) -> int:
+        if self.string_keys:
+            return self.max_groups + 1
         v = C.c_int64()
         capi.check(capi.lib().qdb_gb_max_hash_count(self.table.handle, C.byref(v)))
         return v.value
@@ -350,6 +360,10 @@ class GPUGroupBy:
         """(outKeys, outValues, outDataElementCount, outKeysNullMask, outValuesNullMask); outKeys is a list of
         DeviceBuffers for the multi-key form.  outValues is None for AGG none."""
         aggs = [] if self.agg == "none" else [self.agg]
+        if self.string_keys:
+            keys, knull, vals, n = self.table.results(aggs)
+            v, vn = vals.get(self.agg, (None, None))
+            return keys, v, n, knull, vn
         keys, knulls, vals, n = self.table.results(aggs)
         if self.agg == "count" and n:
             # COUNT is never NULL: the reference allocates an all-zero mask (GPUGroupBy.cuh:571-583).
@@ -484,3 +498,181 @@ def order_by(cols: Sequence[torch.Tensor], descending: Optional[Sequence[bool]] 
     desc = (C.c_int32 * k)(*[int(bool(d)) for d in (descending or [False] * k)])
     capi.check(capi.lib().qdb_order_by(k, types, ptrs, nl, desc, n, _ptr(out), _stream(stream)))
     return out[:n]
+
+
+class GPUString:
+    """GPUMemory::GPUString (qikkDB/QueryEngine/GPUCore/GPUMemory.cuh): `allChars` every string's characters
+    concatenated (uint8), `stringIndices` the int64 end offset of each string (string i is
+    allChars[stringIndices[i-1] if i else 0 : stringIndices[i]]).  Either member is a torch CUDA tensor or a
+    DeviceBuffer."""
+
+    def __init__(self, allChars, stringIndices):
+        self.allChars = allChars
+        self.stringIndices = stringIndices
+
+    @staticmethod
+    def from_strings(strings, device="cuda") -> "GPUString":
+        """StringFactory::PrepareGPUString: uploads a list of str/bytes (None stands for an empty string)."""
+        bs = [b"" if x is None else (x.encode() if isinstance(x, str) else bytes(x)) for x in strings]
+        ends = np.cumsum(np.fromiter((len(b) for b in bs), dtype=np.int64, count=len(bs)), dtype=np.int64)
+        chars = np.frombuffer(b"".join(bs), dtype=np.uint8).copy()
+        return GPUString(torch.from_numpy(chars).to(device), torch.from_numpy(ends).to(device))
+
+    def __len__(self) -> int:
+        x = self.stringIndices
+        return x.numel() if isinstance(x, torch.Tensor) else x.count
+
+    def to_strings(self) -> list:
+        """GPUReconstruct::ReconstructStringCol to host: the strings as bytes."""
+        def host(x):
+            return x.cpu().numpy() if isinstance(x, torch.Tensor) else x.numpy()
+        ends = host(self.stringIndices) if len(self) else np.zeros(0, dtype=np.int64)
+        chars = host(self.allChars) if len(self) and int(ends[-1]) else np.zeros(0, dtype=np.uint8)
+        out, b = [], 0
+        for e in ends:
+            out.append(chars[b:int(e)].tobytes())
+            b = int(e)
+        return out
+
+
+class StringGroupByTable:
+    """A multi-aggregate GROUP BY table over string keys (qdb_gbs_*)."""
+
+    def __init__(self, aggs: Sequence[str], val_dtype, max_groups: int, max_key_bytes: int = 0, stream=None):
+        self.aggs = [a for a in aggs if a != "none"]
+        self.val_code = type_code(val_dtype) if val_dtype is not None else 0
+        mask = 0
+        for a in self.aggs:
+            mask |= AGG_CODES[a]
+        h = C.c_void_p()
+        capi.check(capi.lib().qdb_gbs_create(C.byref(h), mask, self.val_code, int(max_groups), int(max_key_bytes),
+                                             _stream(stream)))
+        self.handle = h
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) and self.handle.value:
+                capi.lib().qdb_gbs_destroy(self.handle)
+                self.handle = C.c_void_p()
+        except Exception:
+            pass
+
+    def process(self, keys: GPUString, values=None, n: Optional[int] = None, key_nulls=None, value_nulls=None,
+                mask=None, stream=None, sync: bool = True) -> None:
+        n = len(keys) if n is None else n
+        capi.check(capi.lib().qdb_gbs_process(self.handle, _ptr(keys.allChars), _ptr(keys.stringIndices),
+                                              _ptr(key_nulls), _ptr(values), _ptr(value_nulls), _ptr(mask), int(n),
+                                              _stream(stream)))
+        if sync:
+            self.check(stream)
+
+    def check(self, stream=None) -> None:
+        capi.check(capi.lib().qdb_gbs_check(self.handle, _stream(stream)))
+
+    def reset(self, stream=None) -> None:
+        capi.check(capi.lib().qdb_gbs_reset(self.handle, _stream(stream)))
+
+    def results(self, aggs: Optional[Sequence[str]] = None, stream=None):
+        """(keys: GPUString of DeviceBuffers, key_nulls: DeviceBuffer, {agg: (values, nulls)}, count)."""
+        aggs = list(self.aggs if aggs is None else aggs)
+        na = len(aggs)
+        codes = (C.c_int32 * max(na, 1))(*[AGG_CODES[a] for a in aggs])
+        ov = (C.c_void_p * max(na, 1))()
+        ovn = (C.c_void_p * max(na, 1))()
+        oc, oe, okn = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        cnt = C.c_int64()
+        capi.check(capi.lib().qdb_gbs_results(self.handle, na, codes, C.byref(oc), C.byref(oe), C.byref(okn),
+                                              ov if na else None, ovn if na else None, C.byref(cnt), _stream(stream)))
+        n = cnt.value
+        ends = DeviceBuffer(oe.value, n, np.int64)
+        nchars = int(ends.numpy()[-1]) if n else 0
+        keys = GPUString(DeviceBuffer(oc.value, nchars, np.uint8), ends)
+        vals = {}
+        vdt = CODE_TO_NP.get(self.val_code, np.int64)
+        for i, a in enumerate(aggs):
+            vals[a] = (DeviceBuffer(ov[i], n, np.int64 if a == "count" else vdt),
+                       DeviceBuffer(ovn[i], nullmask_words(n), np.uint64))
+        return keys, DeviceBuffer(okn.value, nullmask_words(n), np.uint64), vals, n
+
+    def results_host(self, aggs: Optional[Sequence[str]] = None, stream=None) -> dict:
+        """{key bytes, or None for the NULL key: {agg: value, or None for a NULL aggregate}}."""
+        keys, knull, vals, n = self.results(aggs, stream)
+        ks = keys.to_strings()
+        kn = unpack_nullmask(knull.numpy(), n) if n else np.zeros(0, dtype=bool)
+        host = {a: (v.numpy(), unpack_nullmask(vn.numpy(), n)) for a, (v, vn) in vals.items()} if n else {}
+        out = {}
+        for i in range(n):
+            key = None if kn[i] else ks[i]
+            assert key not in out, f"duplicate group {key!r}"
+            out[key] = {a: (None if (a != "count" and hv[1][i]) else hv[0][i].item()) for a, hv in host.items()}
+        return out
+
+
+class ScalarAggregate:
+    """Scalar aggregation over a query's blocks (qdb_scalar_*): COUNT, SUM, MIN, MAX (and AVG) of one value column,
+    filtered by an optional `col OP constant` predicate and mask, NULL values skipped."""
+
+    def __init__(self, val_dtype, stream=None):
+        h = C.c_void_p()
+        self.val_code = type_code(val_dtype)
+        capi.check(capi.lib().qdb_scalar_create(C.byref(h), self.val_code, _stream(stream)))
+        self.handle = h
+
+    def __del__(self):
+        try:
+            if self.handle:
+                capi.lib().qdb_scalar_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    def reset(self, stream=None) -> None:
+        capi.check(capi.lib().qdb_scalar_reset(self.handle, _stream(stream)))
+
+    def process(self, values: torch.Tensor, n: Optional[int] = None, value_nulls=None, pred=None, mask=None,
+                stream=None) -> None:
+        n = values.numel() if n is None else n
+        capi.check(capi.lib().qdb_scalar_process(self.handle, _ptr(values), _ptr(value_nulls), int(n),
+                                                 C.byref(pred) if pred is not None else None, _ptr(mask),
+                                                 _stream(stream)))
+
+    def result(self, agg: str, stream=None):
+        """The aggregate as a Python number, or None for MIN/MAX/SUM/AVG over no row."""
+        code = CODE_TO_NP[self.val_code] if agg != "count" else np.int64
+        out = np.zeros(1, dtype=code)
+        isnull = C.c_int32()
+        capi.check(capi.lib().qdb_scalar_result(self.handle, AGG_CODES[agg], out.ctypes.data, C.byref(isnull),
+                                                _stream(stream)))
+        return None if isnull.value else out[0].item()
+
+
+class GPUAggregation:
+    """GPUAggregation::col<AGG, OUT, IN> (qikkDB/QueryEngine/GPUCore/GPUAggregation.cuh:15-37): one aggregate of a
+    whole column (here optionally filtered and with NULL values skipped)."""
+
+    @staticmethod
+    def col(agg: str, ACol: torch.Tensor, dataElementCount: int, nullMask=None, pred=None, mask=None, stream=None):
+        a = ScalarAggregate(ACol.dtype, stream)
+        a.process(ACol, dataElementCount, nullMask, pred, mask, stream)
+        return a.result(agg, stream)
+
+
+def block_may_pass(pred_dtype, op: int, constant, const_dtype, block_min, block_max) -> bool:
+    """qdb_pred_block_may_pass: whether a block whose predicate column spans [block_min, block_max] can hold a row
+    passing `col OP constant` (GpuSqlDispatcher::WhereEvaluation's block skipping)."""
+    p = capi.qdb_pred()
+    p.col = 1  # not read: only the type, op and constant matter here
+    p.type = type_code(pred_dtype)
+    p.op = op
+    ct = type_code(const_dtype)
+    p.const_type = ct
+    if ct in (capi.QDB_FLOAT, capi.QDB_DOUBLE):
+        p.const_f = float(np.float32(constant)) if ct == capi.QDB_FLOAT else float(constant)
+    else:
+        p.const_i = int(constant)
+    npdt = CODE_TO_NP[p.type]
+    lo = np.array([block_min], dtype=npdt)
+    hi = np.array([block_max], dtype=npdt)
+    m = C.c_int32()
+    capi.check(capi.lib().qdb_pred_block_may_pass(C.byref(p), lo.ctypes.data, hi.ctypes.data, C.byref(m)))
+    return bool(m.value)

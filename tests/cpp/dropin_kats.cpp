@@ -12,7 +12,8 @@
 //   then the key columns, the key null flags (when given), the values, the value null flags and the predicate
 //   column (when given), <rows> numbers each.
 // Output, per case:  "result <name> <groups> <multiplier>", then per group "<key...> <key null...> <value null> <value>".
-// With the single argument "version" it prints the library version and exits (no GPU needed).
+// With the single argument "version" it prints the library version and exits (no GPU needed); "order", "scalar" and
+// "string" run the ORDER BY, scalar-aggregation and string-key GROUP BY operators (described at their functions).
 #include <cstdint>
 #include <algorithm>
 #include <cstdio>
@@ -245,10 +246,179 @@ void run(const Case& c) {
 
 }  // namespace
 
+// "order" mode: GROUP BY SUM then ORDER BY key or value (DispatcherGroupByTests.cpp:1551-1588) through
+// GPUGroupBy + GPUOrderBy::OrderByColumn + GPUOrderBy::ReOrderByIdx.  Input per case: "ocase <name> <by_value> <desc>
+// <rows>", the keys, the values.  Output: "oresult <name> <groups>" and one "<key> <sum>" line per group, in order.
+int run_order() {
+    std::string tag, name;
+    while (std::cin >> tag) {
+        int by_value = 0, desc = 0;
+        int32_t n = 0;
+        std::cin >> name >> by_value >> desc >> n;
+        std::vector<int32_t> k(n), v(n);
+        for (auto& x : k) std::cin >> x;
+        for (auto& x : v) std::cin >> x;
+        cuda_ptr<int32_t> dk = device_col(k, 0, n), dv = device_col(v, 0, n);
+        GPUGroupBy<AggregationFunctions::sum, int32_t, int32_t, int32_t> gb(1024, 1);
+        gb.ProcessBlock(dk.get(), dv.get(), n);
+        int32_t *keys = nullptr, *sums = nullptr, g = 0;
+        gb.GetResults(&keys, &sums, &g);
+        GPUOrderBy ob(g);
+        cuda_ptr<int32_t> idx(static_cast<size_t>(g > 0 ? g : 1));
+        ob.OrderByColumn(idx.get(), by_value ? sums : keys, nullptr, g, desc ? OrderBy::DESC : OrderBy::ASC);
+        cuda_ptr<int32_t> ok(static_cast<size_t>(g > 0 ? g : 1)), os(static_cast<size_t>(g > 0 ? g : 1));
+        GPUOrderBy::ReOrderByIdx(ok.get(), idx.get(), keys, g);
+        GPUOrderBy::ReOrderByIdx(os.get(), idx.get(), sums, g);
+        std::vector<int32_t> hk = to_host(ok.get(), g), hs = to_host(os.get(), g);
+        std::printf("oresult %s %d\n", name.c_str(), g);
+        for (int32_t i = 0; i < g; ++i) std::printf("%d %d\n", hk[i], hs[i]);
+        GPUMemory::free(keys);
+        GPUMemory::free(sums);
+    }
+    return 0;
+}
+
+// "scalar" mode: the aggregates of GPUAggregationTests.cu (min, max, sum, avg, count of one column) through
+// GPUAggregation::col.  Input: "<type code> <rows>" then the values.  Output: "<min> <max> <sum> <avg> <count>".
+template <typename T>
+void scalar_case(int32_t n) {
+    std::vector<T> v(n);
+    for (auto& x : v) std::cin >> x;
+    cuda_ptr<T> d = device_col(v, 0, n);
+    cuda_ptr<T> out(4);
+    cuda_ptr<int64_t> cnt(1);
+    GPUAggregation::col<AggregationFunctions::min>(out.get(), d.get(), n);
+    GPUAggregation::col<AggregationFunctions::max>(out.get() + 1, d.get(), n);
+    GPUAggregation::col<AggregationFunctions::sum>(out.get() + 2, d.get(), n);
+    GPUAggregation::col<AggregationFunctions::avg>(out.get() + 3, d.get(), n);
+    GPUAggregation::col<AggregationFunctions::count>(cnt.get(), d.get(), n);
+    std::vector<T> h = to_host(out.get(), 4);
+    std::vector<int64_t> c = to_host(cnt.get(), 1);
+    std::cout.precision(17);
+    std::cout << h[0] << " " << h[1] << " " << h[2] << " " << h[3] << " " << c[0] << "\n";
+}
+
+int run_scalar() {
+    int32_t type = 0, n = 0;
+    while (std::cin >> type >> n) {
+        if (type == COLUMN_INT) scalar_case<int32_t>(n);
+        else if (type == COLUMN_LONG) scalar_case<int64_t>(n);
+        else if (type == COLUMN_FLOAT) scalar_case<float>(n);
+        else scalar_case<double>(n);
+    }
+    return 0;
+}
+
+// "string" mode: GROUP BY over string keys (GPUGroupByTests.cu:474-516, DispatcherGroupByTests.cpp:1422-1467,
+// DispatcherNullTests.cpp:1372-1750) through GPUGroupBy<AGG, O, std::string, int32_t>, block by block.  Input per
+// case: "scase <name> <agg> <blocks>", then per block "<rows>" and per row "<key> <value> <keep>": key N (NULL),
+// - (empty) or the bytes in hex; value N (NULL), X (no value column) or an integer; keep 0 drops the row before
+// the block is built, as the dispatcher's WHERE compaction does.  Output: "sresult <name> <groups>" and one
+// "<key> <value>" line per group (value N for a NULL aggregate).
+template <typename AGG, typename O>
+void string_case(const std::string& name, int32_t blocks) {
+    GPUGroupBy<AGG, O, std::string, int32_t> gb(8, 1);
+    for (int32_t b = 0; b < blocks; ++b) {
+        int32_t rows = 0;
+        std::cin >> rows;
+        std::string chars;
+        std::vector<int64_t> ends;
+        std::vector<int32_t> vals;
+        std::vector<nullmask_t> kn(GPUMemory::CalculateNullMaskSize(rows) + 1, 0), vn(kn.size(), 0);
+        bool any_kn = false, any_vn = false, have_vals = true;
+        for (int32_t r = 0; r < rows; ++r) {
+            std::string k, v;
+            int keep = 1;
+            std::cin >> k >> v >> keep;
+            if (!keep) continue;
+            const size_t i = ends.size();
+            if (k == "N") {
+                kn[i / 64] |= nullmask_t(1) << (i % 64);
+                any_kn = true;
+            } else if (k != "-") {
+                for (size_t c = 0; c + 1 < k.size(); c += 2) chars.push_back(static_cast<char>(std::stoi(k.substr(c, 2), nullptr, 16)));
+            }
+            ends.push_back(static_cast<int64_t>(chars.size()));
+            if (v == "X") have_vals = false;
+            else if (v == "N") {
+                vn[i / 64] |= nullmask_t(1) << (i % 64);
+                any_vn = true;
+                vals.push_back(0);
+            } else {
+                vals.push_back(std::stoi(v));
+            }
+        }
+        const int32_t n = static_cast<int32_t>(ends.size());
+        if (n == 0) continue;
+        cuda_ptr<char> dc(chars.size() + 1);
+        if (!chars.empty()) GPUMemory::copyHostToDevice(dc.get(), chars.data(), chars.size());
+        cuda_ptr<int64_t> de = device_col(ends, 0, n);
+        cuda_ptr<nullmask_t> dkn = device_col(kn, 0, static_cast<int32_t>(kn.size()));
+        cuda_ptr<nullmask_t> dvn = device_col(vn, 0, static_cast<int32_t>(vn.size()));
+        cuda_ptr<int32_t> dv(have_vals ? static_cast<size_t>(n) : 1);
+        if (have_vals) GPUMemory::copyHostToDevice(dv.get(), vals.data(), static_cast<size_t>(n));
+        gb.ProcessBlock(GPUMemory::GPUString{dc.get(), de.get()}, have_vals ? dv.get() : nullptr, n,
+                        any_kn ? dkn.get() : nullptr, any_vn ? dvn.get() : nullptr);
+    }
+    GPUMemory::GPUString keys{nullptr, nullptr};
+    O* vals = nullptr;
+    nullmask_t *kn = nullptr, *vn = nullptr;
+    int32_t g = 0;
+    gb.GetResults(&keys, &vals, &g, &kn, &vn);
+    std::printf("sresult %s %d\n", name.c_str(), g);
+    if (g > 0) {
+        std::vector<int64_t> ends = to_host(keys.stringIndices, g);
+        std::string chars(static_cast<size_t>(ends[g - 1]), '\0');
+        if (!chars.empty()) GPUMemory::copyDeviceToHost(&chars[0], keys.allChars, chars.size());
+        std::vector<O> hv = to_host(vals, g);
+        std::vector<nullmask_t> hkn = to_host(kn, static_cast<int32_t>(GPUMemory::CalculateNullMaskSize(g)));
+        std::vector<nullmask_t> hvn = to_host(vn, static_cast<int32_t>(GPUMemory::CalculateNullMaskSize(g)));
+        for (int32_t i = 0; i < g; ++i) {
+            const int64_t b0 = i ? ends[i - 1] : 0;
+            std::string key;
+            if ((hkn[i / 64] >> (i % 64)) & 1) key = "N";
+            else if (ends[i] == b0) key = "-";
+            else
+                for (int64_t c = b0; c < ends[i]; ++c) {
+                    char hx[3];
+                    std::snprintf(hx, sizeof(hx), "%02x", static_cast<unsigned char>(chars[static_cast<size_t>(c)]));
+                    key += hx;
+                }
+            if ((hvn[i / 64] >> (i % 64)) & 1) std::printf("%s N\n", key.c_str());
+            else std::printf("%s %lld\n", key.c_str(), static_cast<long long>(hv[i]));
+        }
+    }
+    GPUMemory::free(keys);
+    GPUMemory::free(vals);
+    GPUMemory::free(kn);
+    GPUMemory::free(vn);
+}
+
+int run_string() {
+    std::string tag, name, agg;
+    int32_t blocks = 0;
+    while (std::cin >> tag >> name >> agg >> blocks) {
+        if (agg == "sum") string_case<AggregationFunctions::sum, int32_t>(name, blocks);
+        else if (agg == "min") string_case<AggregationFunctions::min, int32_t>(name, blocks);
+        else if (agg == "max") string_case<AggregationFunctions::max, int32_t>(name, blocks);
+        else if (agg == "avg") string_case<AggregationFunctions::avg, int32_t>(name, blocks);
+        else string_case<AggregationFunctions::count, int64_t>(name, blocks);
+    }
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc > 1 && std::string(argv[1]) == "version") {
         std::printf("%s\n", qdb_version());
         return 0;
+    }
+    try {
+        if (argc > 1 && std::string(argv[1]) == "order") return run_order();
+        if (argc > 1 && std::string(argv[1]) == "scalar") return run_scalar();
+        if (argc > 1 && std::string(argv[1]) == "string") return run_string();
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
+        return 2;
     }
     try {
         Case c;

@@ -196,7 +196,67 @@ order_cases.append({"name": "IntegerSimpleSumOrderByValues", "source": DGB + ":1
                     "values": list(range(len(OBK))), "order_by": "value", "descending": False,
                     "expected": [[10, 1], [2, 5], [6, 9], [4, 13], [8, 17]]})
 
+# GROUP BY over string keys.  blocks: the row blocks the test processes one ProcessBlock each; keys None = NULL;
+# values None = NULL (values absent: COUNT of the key column, i.e. of rows); expected: (key or None, value or None).
+string_cases = []
+
+
+def gbs(name, src, agg, blocks_keys, blocks_vals, expected, pred_gt=None):
+    string_cases.append({"name": name, "source": src, "agg": agg, "blocks_keys": blocks_keys,
+                         "blocks_values": blocks_vals, "pred_values_greater": pred_gt,
+                         "expected": [{"key": k, "value": v} for k, v in expected]})
+
+
+gbs("StringUnique", GGB + ":474", "sum", [["Apple", "Abcd", "XYZ"]], [[1, 2, -1]],
+    [("Apple", 1), ("Abcd", 2), ("XYZ", -1)])
+gbs("StringSimple", GGB + ":480", "sum", [["Apple", "Abcd", "XYZ", "Abcd", "ZYX", "XYZ"]], [[1, 2, -1, 3, 7, 5]],
+    [("Apple", 1), ("Abcd", 5), ("XYZ", 4), ("ZYX", 7)])
+gbs("StringMultiBlockSimple", GGB + ":487", "sum",
+    [["Apple", "Abcd"], ["XYZ", "Abcd"], ["ZYX", "XYZ"], ["Apple", "Apple"]], [[1, 1], [1, 2], [1, 2], [2, 4]],
+    [("Apple", 7), ("Abcd", 3), ("XYZ", 3), ("ZYX", 1)])
+MBK = [["Apple", "Abcd", "Apple", "XYZ"], ["Banana", "XYZ", "Abcd", "0"], ["XYZ", "XYZ"]]
+MBV = [[1, 2, 3, 4], [5, 6, 7, 10], [13, 15]]
+gbs("StringMultiBlockMediumSum", GGB + ":494", "sum", MBK, MBV,
+    [("Apple", 4), ("Abcd", 9), ("Banana", 5), ("XYZ", 38), ("0", 10)])
+gbs("StringMultiBlockMediumMin", GGB + ":502", "min", MBK, MBV,
+    [("Apple", 1), ("Abcd", 2), ("Banana", 5), ("XYZ", 4), ("0", 10)])
+gbs("StringMultiBlockMediumMax", GGB + ":510", "max", MBK, MBV,
+    [("Apple", 3), ("Abcd", 7), ("Banana", 5), ("XYZ", 15), ("0", 10)])
+SK = ["Apple", "Abcd", "Apple", "XYZ", "Banana", "XYZ", "Abcd", "0", "XYZ", "XYZ"]
+SV = [1, 2, 3, 4, 5, 6, 7, 10, 13, 15]
+gbs("StringSimpleSum", DGB + ":1422", "sum", [SK], [SV],
+    [("Apple", 4), ("Abcd", 9), ("Banana", 5), ("XYZ", 38), ("0", 10)])
+gbs("StringSimpleMin", DGB + ":1429", "min", [SK], [SV],
+    [("Apple", 1), ("Abcd", 2), ("Banana", 5), ("XYZ", 4), ("0", 10)])
+gbs("StringSimpleMax", DGB + ":1436", "max", [SK], [SV],
+    [("Apple", 3), ("Abcd", 7), ("Banana", 5), ("XYZ", 15), ("0", 10)])
+gbs("StringSimpleAvg", DGB + ":1443", "avg", [SK], [SV],
+    [("Apple", 2), ("Abcd", 4), ("Banana", 5), ("XYZ", 9), ("0", 10)])
+gbs("StringSimpleCount", DGB + ":1450", "count", [SK], [SV],
+    [("Apple", 2), ("Abcd", 2), ("Banana", 1), ("XYZ", 4), ("0", 1)])
+gbs("StringSimpleCountStringWhere", DGB + ":1457", "count", [SK], None, [("Abcd", 1), ("XYZ", 3), ("0", 1)],
+    pred_gt={"values": [SV], "const": 5})
+gbs("StringSimpleCountString", DGB + ":1463", "count", [SK], None,
+    [("Apple", 2), ("Abcd", 2), ("Banana", 1), ("XYZ", 4), ("0", 1)])
+
+
+def null_rows(n, key_of, null_key, null_val):
+    keys = [None if null_key(i) else key_of(i) for i in range(n)]
+    vals = [None if null_val(i) else 2 for i in range(n)]
+    return [keys[b:b + 8] for b in range(0, n, 8)], [vals[b:b + 8] for b in range(0, n, 8)]
+
+
+# DispatcherNullTests.cpp:1372-1456: 32 rows in blocks of 8, key i%4 (2: NULL), value 2.
+nk, nv = null_rows(32, lambda i: ["Apple", "Nut", None, "XYZ"][i % 4], lambda i: i % 4 == 2, lambda i: False)
+gbs("GroupByStringNullKeySum", DNT + ":1372", "sum", nk, nv, [(None, 16), ("Apple", 16), ("Nut", 16), ("XYZ", 16)])
+# DispatcherNullTests.cpp:1458-1750: 24 rows in blocks of 8, value NULL where (i%4 == 2 and i < 8) or i%4 == 3.
+vk, vv = null_rows(24, lambda i: ["Apple", "Nut", "Straw", "car0"][i % 4], lambda i: False,
+                   lambda i: (i % 4 == 2 and i < 8) or i % 4 == 3)
+gbs("GroupByStringNullValueSum", DNT + ":1458", "sum", vk, vv, [("Apple", 12), ("Nut", 12), ("Straw", 8), ("car0", None)])
+gbs("GroupByStringNullValueAvg", DNT + ":1558", "avg", vk, vv, [("Apple", 2), ("Nut", 2), ("Straw", 2), ("car0", None)])
+gbs("GroupByStringNullValueCount", DNT + ":1654", "count", vk, vv, [("Apple", 6), ("Nut", 6), ("Straw", 4), ("car0", 0)])
+
 with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
-    json.dump({"generated_by": "tests/golden/make_kats.py", "cases": cases, "order_by_cases": order_cases}, f,
-              indent=1)
-print(len(cases), "cases,", len(order_cases), "ORDER BY cases")
+    json.dump({"generated_by": "tests/golden/make_kats.py", "cases": cases, "order_by_cases": order_cases,
+               "string_cases": string_cases}, f, indent=1)
+print(len(cases), "cases,", len(order_cases), "ORDER BY cases,", len(string_cases), "string cases")

@@ -52,3 +52,31 @@ def result_map(keys, key_nulls, values, value_nulls):
         assert key not in out, f"duplicate group {key}"
         out[key] = v
     return out
+
+
+def load_string_kats():
+    with open(os.path.join(HERE, "golden", "reference_kats.json")) as f:
+        return json.load(f)["string_cases"]
+
+
+def string_blocks(case):
+    """Per block: (key strings with None for NULL, values np.int32 or None, value NULL flags or None, mask or None)."""
+    out = []
+    pv = case.get("pred_values_greater")
+    for b, keys in enumerate(case["blocks_keys"]):
+        vals = vn = None
+        if case["blocks_values"] is not None:
+            raw = case["blocks_values"][b]
+            vn = np.array([v is None for v in raw], dtype=bool)
+            vals = np.array([0 if v is None else v for v in raw], dtype=np.int32)
+            if not vn.any():
+                vn = None
+        mask = None
+        if pv is not None:
+            mask = (np.asarray(pv["values"][b], dtype=np.int32) > pv["const"]).astype(np.int8)
+        out.append((keys, vals, vn, mask))
+    return out
+
+
+def string_expected(case):
+    return {(None if e["key"] is None else e["key"].encode()): e["value"] for e in case["expected"]}

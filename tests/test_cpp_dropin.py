@@ -104,3 +104,79 @@ def test_dropin_runs_reference_kats(cuda):
         if c["agg"] == "none":
             exp = {k: None for k in exp}
         assert groups == exp, f"{c['name']}: {groups} != {exp}"
+
+
+@pytest.mark.gpu
+def test_dropin_order_by_and_scalar_aggregation(cuda):
+    """GPUOrderBy over GROUP BY results (DispatcherGroupByTests.cpp:1551-1588) and GPUAggregation::col on the inputs
+    of GPUAggregationTests.cu:13-126 (2^18 default-seeded int32 draws as int32 and int64 columns, 0.25 as float),
+    through the C++ drop-in."""
+    import json
+
+    import oracle
+    exe = build_program()
+    with open(os.path.join(ROOT, "tests", "golden", "reference_kats.json")) as f:
+        cases = json.load(f)["order_by_cases"]
+    text = ""
+    for c in cases:
+        text += f"ocase {c['name']} {int(c['order_by'] == 'value')} {int(c['descending'])} {len(c['keys'])}\n"
+        text += " ".join(map(str, c["keys"])) + "\n" + " ".join(map(str, c["values"])) + "\n"
+    r = subprocess.run([exe, "order"], input=text, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    i = 0
+    for c in cases:
+        tag, name, g = lines[i].split()
+        assert tag == "oresult" and name == c["name"]
+        got = [[int(x) for x in line.split()] for line in lines[i + 1:i + 1 + int(g)]]
+        assert got == c["expected"], (name, got)
+        i += 1 + int(g)
+
+    n = 1 << 18
+    a32, _ = oracle.reference_filter_inputs(np.int32, 1, n)
+    a64, _ = oracle.reference_filter_inputs(np.int64, 1, n)
+    f32 = np.full(n, 0.25, dtype=np.float32)
+    text = "\n".join(f"{code} {n}\n" + " ".join(map(str, arr.tolist()))
+                     for code, arr in ((8, a32), (9, a64), (10, f32))) + "\n"
+    r = subprocess.run([exe, "scalar"], input=text, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = [line.split() for line in r.stdout.splitlines()]
+    # the test's own expectations: T sum (int32 wraps), avg = sum / N truncated, cnt = N
+    s32 = (int(a32.astype(np.int64).sum()) + (1 << 31)) % (1 << 32) - (1 << 31)
+    assert [int(x) for x in out[0]] == [int(a32.min()), int(a32.max()), s32, int(s32 / n), n]
+    s64 = int(a64.sum())
+    assert [int(x) for x in out[1]] == [int(a64.min()), int(a64.max()), s64, int(s64 / n), n]
+    assert [float(x) for x in out[2]] == [0.25, 0.25, 0.25 * n, 0.25, n]
+
+
+@pytest.mark.gpu
+def test_dropin_string_groupby(cuda):
+    """GPUGroupBy<AGG, O, std::string, int32_t> through the C++ drop-in on the reference's string GROUP BY tests
+    (GPUGroupByTests.cu:474-516, DispatcherGroupByTests.cpp:1422-1467, DispatcherNullTests.cpp:1372-1750)."""
+    from kat_util import load_string_kats, string_blocks, string_expected
+    exe = build_program()
+    cases = load_string_kats()
+    text = ""
+    for c in cases:
+        blocks = string_blocks(c)
+        text += f"scase {c['name']} {c['agg']} {len(blocks)}\n"
+        for keys, vals, vn, mask in blocks:
+            text += f"{len(keys)}\n"
+            for i, k in enumerate(keys):
+                kt = "N" if k is None else ("-" if k == "" else k.encode().hex())
+                vt = "X" if vals is None else ("N" if vn is not None and vn[i] else str(int(vals[i])))
+                text += f"{kt} {vt} {1 if mask is None else int(mask[i])}\n"
+    r = subprocess.run([exe, "string"], input=text, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    i = 0
+    for c in cases:
+        tag, name, g = lines[i].split()
+        assert tag == "sresult" and name == c["name"]
+        got = {}
+        for line in lines[i + 1:i + 1 + int(g)]:
+            k, v = line.split()
+            key = None if k == "N" else (b"" if k == "-" else bytes.fromhex(k))
+            got[key] = None if v == "N" else int(v)
+        assert got == string_expected(c), (name, got)
+        i += 1 + int(g)
