@@ -15,8 +15,10 @@ merged (weak scaling).  `e2e` measures the same query through the C ABI from pin
 
 On one GPU the same line also carries the other configurations, each measured after the headline:
 `plain_1m` (2^20 rows, int32 keys over 1000 values, cold and warm), `composite_128m` (2^27 rows, 4096 x 4096
-composite keys), `batched` (4096 instances in one CUDA graph against the plain path looped in C) and `served`
-(continuous batching over 2^30 resident rows at four Poisson rates); --headline-only skips them.
+composite keys), `batched` (4096 instances in one CUDA graph against the plain path looped in C), `served`
+(continuous batching over 2^30 resident rows at four Poisson rates), and the operators next to the path:
+`scalar_256m` (the filtered workload's WHERE and values without GROUP BY), `string_32m` (GROUP BY over 2^25 string
+keys) and `order_by_groups` (ORDER BY SUM DESC of the string GROUP BY's groups); --headline-only skips them.
 
 --impl reference times the reference's CPU-side GROUP BY (the hash-map aggregation its tests check against,
 restated in oracle/) on all host threads over the same workload.
@@ -65,10 +67,11 @@ def parse_args():
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the plain, composite, batched and served sub-workloads of the default run")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="filtered", choices=["filtered", "batched", "served", "plain", "composite"])
+    ap.add_argument("--workload", default="filtered",
+                    choices=["filtered", "batched", "served", "plain", "composite", "scalar", "string"])
     ap.add_argument("--composite-rows", type=int, default=1 << 27)
     ap.add_argument("--no-oracle", action="store_true",
-                    help="plain / composite on their own: skip the oracle leg (profiling runs)")
+                    help="plain / composite / scalar / string on their own: skip the oracle leg (profiling runs)")
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="batched / served: queries of the one-by-one plain-path comparison (0 = all / 24)")
@@ -385,6 +388,10 @@ def run_ours(args):
         subs["batched"] = batched_measure(args, dev, sub=True)
         torch.cuda.empty_cache()
         subs["served"] = served_measure(args, dev, sub=True)
+        torch.cuda.empty_cache()
+        subs["scalar_256m"] = scalar_measure(args, dev)
+        torch.cuda.empty_cache()
+        subs["string_32m"], subs["order_by_groups"] = string_and_order_measure(args, dev)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -527,6 +534,167 @@ def c2_measure(args, dev) -> dict:
                            "sample": f"all {n} rows, hash-map GROUP BY, {r['threads']} threads, {r['seconds']:.1f} s"}
     out["parity"] = _exact_parity(g, r, aggs)
     return out
+
+
+# ---------------------------------------------------------------------------------------------------------------
+# The operators next to the path: scalar aggregation, GROUP BY over string keys, ORDER BY of GROUP BY results.
+# ---------------------------------------------------------------------------------------------------------------
+SCALAR_WORKLOAD = ("scalar-256M: 2^28 rows, SUM+COUNT+MIN+MAX of f32 lognormal(2,1) values WHERE f32 U[0,1) < 0.5 "
+                   "(the filtered workload's predicate and value columns, no GROUP BY)")
+STR_SEED = 20240606
+STR_WORKLOAD = ("string-groupby-32M: 2^25 rows, string keys Zipf(1.1) over 1M distinct strings of 8-24 bytes "
+                "('c' + 7 digits + '#' padding; GPUString layout: characters + int64 end offsets), int32 value "
+                "uniform in [-1000,1000]; SUM+COUNT")
+OB_WORKLOAD = "order-by-sum-desc: ORDER BY SUM(value) DESC of the string GROUP BY's groups (int32 column, no NULLs)"
+
+
+def scalar_measure(args, dev) -> dict:
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import FilterConditions, ScalarAggregate, make_pred
+    n = args.rows
+    p = dg.uniform_f32(SEED, 0, n)
+    v = dg.lognormal_f32(SEED, 2, n, 2.0, 1.0)
+    dp, dv = torch.from_numpy(p).to(dev), torch.from_numpy(v).to(dev)
+    pred = make_pred(dp, FilterConditions.less, 0.5, np.float32)
+    acc = ScalarAggregate(np.float32)
+
+    def step():
+        acc.reset()
+        acc.process(dv, n, pred=pred)
+
+    ms = statistics.median(_event_steps(step, args.steps, args.warmup))
+    got = {a: acc.result(a) for a in ("sum", "count", "min", "max")}
+    peak, peak_kind = measured_peak()
+    out = {"workload": SCALAR_WORKLOAD, "metric": "scalar aggregation rows/s", "unit": "rows/s",
+           "value": n / (ms / 1e3), "ms_per_step": ms, "step": "reset + one fused filter/reduce launch",
+           "l2": "inputs (2.1 GB) > L2, no flush",
+           "roofline": {"bound": "hbm", "achieved": n * 8 / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": n * 8 / (ms / 1e3) / 1e9 / peak, "kernel": "scalar_kernel",
+                        "algorithmic_bytes_per_launch": n * 8, "peak_kind": peak_kind}}
+    del dp, dv, pred
+    if getattr(args, "no_oracle", False):
+        return out
+    # cpu_baseline leg: the oracle (a GROUP BY whose keys are all equal has one group) over every row
+    import oracle
+    r = oracle.groupby(np.zeros(n, np.int32), v, pred=(p, FilterConditions.less, 0.5, np.float32, None), threads=0)
+    err = abs(got["sum"] - r["sum"][0]) / abs(r["sum"][0])
+    exact = got["count"] == r["cnt"][0] and got["min"] == r["min"][0] and got["max"] == r["max"][0]
+    out["cpu_baseline"] = {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                           "sample": f"all {n} rows, {r['threads']} threads, {r['seconds']:.2f} s"}
+    out["parity"] = {"checked_against": "oracle over every row", "count_min_max_exact": bool(exact),
+                     "sum_rel_err": err, "parity": bool(exact and err <= FLOAT_RTOL)}
+    return out
+
+
+def string_columns(n: int, n_distinct: int, dev):
+    """Device GPUString columns (characters, end offsets) of n rows whose keys are Zipf(1.1) picks from a vocabulary
+    of n_distinct strings of 8-24 bytes, assembled on the device from the vocabulary."""
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    ids = np.arange(n_distinct, dtype=np.int64)
+    lens = 8 + (ids * 7919) % 17
+    full = np.full((n_distinct, 24), ord("#"), dtype=np.uint8)
+    full[:, 0] = ord("c")
+    for j in range(7):
+        full[:, 1 + j] = ord("0") + (ids // 10 ** (6 - j)) % 10
+    vchars = full[np.arange(24)[None, :] < lens[:, None]]
+    vends = np.cumsum(lens)
+    pick = dg.zipf_i64(STR_SEED, 0, n, n_distinct, 1.1, map_keys=False) - 1
+    dvc = torch.from_numpy(vchars).to(dev)
+    dstart = torch.from_numpy(vends - lens).to(dev)
+    dlen = torch.from_numpy(lens).to(dev)
+    dpick = torch.from_numpy(pick).to(dev)
+    rl = dlen[dpick]
+    ends = torch.cumsum(rl, 0)
+    row = torch.repeat_interleave(torch.arange(n, device=dev), rl)
+    pos = torch.arange(int(ends[-1]), device=dev) - (ends - rl)[row]
+    chars = dvc[dstart[dpick][row] + pos].contiguous()
+    del row, pos, rl
+    return chars, ends.contiguous()
+
+
+def string_and_order_measure(args, dev) -> tuple:
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import GPUString, StringGroupByTable, order_by
+    n, d = 1 << 25, 1 << 20
+    chars, ends = string_columns(n, d, dev)
+    vals_h = dg.uniform_i32(STR_SEED, 1, n, -1000, 1000)
+    vals = torch.from_numpy(vals_h).to(dev)
+    nchars = int(chars.numel())
+    torch.cuda.empty_cache()
+    tab = StringGroupByTable(["sum", "count"], np.int32, d)
+    keys = GPUString(chars, ends)
+    agg_ms = []
+
+    def step():
+        tab.reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tab.process(keys, vals, n, sync=False)
+        e1.record()
+        tab.results(["sum", "count"])
+        agg_ms.append((e0, e1))
+
+    ms = statistics.median(_event_steps(step, args.steps, args.warmup))
+    kms = statistics.median(x.elapsed_time(z) for x, z in agg_ms[args.warmup:])
+    tab.check()
+    alg = nchars + 12 * n
+    peak, peak_kind = measured_peak()
+    s_out = {"workload": STR_WORKLOAD, "metric": "string GROUP BY rows/s", "unit": "rows/s",
+             "value": n / (ms / 1e3), "ms_per_step": ms,
+             "step": "reset + dictionary pass + aggregation pass over slot numbers + GetResults",
+             "roofline": {"bound": "hbm", "achieved": alg / (kms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": alg / (kms / 1e3) / 1e9 / peak, "kernel": "gbs_map_kernel + aggregation pass",
+                          "kernel_ms": kms, "algorithmic_bytes_per_launch": alg,
+                          "bytes_per_row": "key characters + 8 (end offset) + 4 (value)", "peak_kind": peak_kind}}
+
+    # ORDER BY SUM DESC of the groups (the step after the GROUP BY), timed alone
+    _, _, rv, g = tab.results(["sum"])
+    sums = rv["sum"][0].torch()
+    perm_box = []
+    ob_ms = statistics.median(_event_steps(lambda: perm_box.append(order_by([sums], [True])), args.steps,
+                                           args.warmup))
+    perm = perm_box[-1].cpu().numpy()
+    o_out = {"workload": OB_WORKLOAD, "metric": "ORDER BY rows/s", "unit": "rows/s", "rows": int(g),
+             "value": g / (ob_ms / 1e3), "ms_per_step": ob_ms,
+             "step": "qdb_order_by: key encoding, 4 stable radix passes (8-bit digits), permutation",
+             "roofline": {"bound": "hbm", "achieved": g * 4 * 16 / (ob_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                          "frac": g * 4 * 16 / (ob_ms / 1e3) / 1e9 / peak,
+                          "algorithmic_bytes_per_launch": g * 4 * 16,
+                          "note": "4 passes x (key + index read and written) per row; at 1M rows launch-bound",
+                          "peak_kind": peak_kind}}
+    if getattr(args, "no_oracle", False):
+        return s_out, o_out
+    # cpu_baseline legs: the oracle over every row (string ids by first occurrence + hash-map GROUP BY), and its
+    # ORDER BY of the GPU's SUM column; the results check the GPU's bit for bit
+    import oracle
+    hc, he = chars.cpu().numpy(), ends.cpu().numpy()
+    del chars, ends, keys
+    t0 = time.perf_counter()
+    r = oracle.groupby_string(hc, he, vals_h, threads=0)
+    cpu_s = time.perf_counter() - t0
+    got = tab.results_host(["sum", "count"])
+    ok = len(got) == len(r) and all(k in got and got[k]["sum"] == int(st["sum"]) and got[k]["count"] == int(st["cnt"])
+                                    for k, st in r.items())
+    s_out["cpu_baseline"] = {"value": n / cpu_s, "unit": "rows/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"all {n} rows: string ids (1 thread) + hash-map GROUP BY, {cpu_s:.1f} s"}
+    s_out["parity"] = {"checked_against": "oracle over every row", "groups": len(r), "exact": bool(ok),
+                       "parity": bool(ok)}
+    hs = sums.cpu().numpy()
+    t0 = time.perf_counter()
+    operm = oracle.order_by([hs], [True])
+    ob_cpu = time.perf_counter() - t0
+    same = bool((perm == operm).all())
+    o_out["cpu_baseline"] = {"value": g / ob_cpu, "unit": "rows/s", "cores": 1, "kind": "port",
+                             "sample": f"all {g} rows, stable sort, {ob_cpu * 1e3:.1f} ms"}
+    o_out["parity"] = {"checked_against": "oracle stable ORDER BY of the same column", "exact": same, "parity": same}
+    return s_out, o_out
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -920,11 +1088,13 @@ def run_sub(args, fn):
 
 def main():
     args = parse_args()
-    if args.workload in ("plain", "composite"):
+    if args.workload in ("plain", "composite", "scalar", "string"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the headline workload"}))
             return
-        run_sub(args, c0_measure if args.workload == "plain" else c2_measure)
+        fn = {"plain": c0_measure, "composite": c2_measure, "scalar": scalar_measure,
+              "string": lambda a, d: dict(zip(("string_32m", "order_by_groups"), string_and_order_measure(a, d)))}
+        run_sub(args, fn[args.workload])
         return
     if args.workload == "batched":
         if args.impl == "reference":

@@ -286,13 +286,13 @@ int32_t qdb_pred_block_may_pass(const qdb_pred* pred, const void* block_min, con
  * Keys come in the reference's GPUString layout (GPUMemory.cuh GPUString): `chars` all characters concatenated,
  * `ends[i]` the int64 end offset of string i (string i is chars[i ? ends[i-1] : 0, ends[i])).  qdb_gbs_create sizes
  * the table for max_groups distinct non-NULL keys (the NULL key has its own slot, as keyBufferSize_ adds one) and a
- * key arena of max_key_bytes characters (<= 0: 32 per group).  agg_mask as qdb_gb_create; val_type 0 is allowed with
- * QDB_AGG_COUNT only and counts rows.  qdb_gbs_process (asynchronous) aggregates the rows whose `mask` (optional
- * int8, non-zero = keep) is set (a COUNT-only table given no `vals` counts rows); NULL keys (key_nulls, optional)
- * form one group; NULL values (val_nulls, optional)
- * are skipped, a group whose values are all NULL has a NULL aggregate and COUNT 0.  More distinct keys than
- * max_groups, or more key characters than the arena holds, latch QDB_HASH_TABLE_FULL, which qdb_gbs_check (it
- * synchronises `stream`) returns and clears.  qdb_gbs_results (GetResults, GPUGroupByString.cuh:446-563) allocates
+ * key arena of max_key_bytes for the bytes of keys beyond their first 24 (<= 0: 32 per group); a key is at most
+ * 2^20 - 2 bytes long.  agg_mask as qdb_gb_create; val_type 0 is allowed with QDB_AGG_COUNT only and counts rows.
+ * qdb_gbs_process (asynchronous) aggregates the rows whose `mask` (optional int8, non-zero = keep) is set (a
+ * COUNT-only table given no `vals` counts rows); NULL keys (key_nulls, optional) form one group; NULL values
+ * (val_nulls, optional) are skipped, a group whose values are all NULL has a NULL aggregate and COUNT 0.  More
+ * distinct keys than max_groups, or more key bytes than the arena holds, latch QDB_HASH_TABLE_FULL (a longer key
+ * QDB_ERR_TOO_LARGE), which qdb_gbs_check (it synchronises `stream`) returns and clears.  qdb_gbs_results (GetResults, GPUGroupByString.cuh:446-563) allocates
  * the result keys as a GPUString (*out_chars, *out_ends), their NULL bitmask (optional), and per requested aggregate
  * (aggs[n_aggs], n_aggs <= 5) a column typed as qdb_gb_results types it plus its NULL bitmask (optional array);
  * an empty result yields NULL pointers and count 0.  It synchronises `stream`. */

@@ -46,25 +46,39 @@ __global__ void __launch_bounds__(kScThreads) scalar_kernel(const VT* __restrict
     unsigned long long cnt = 0, isum = 0;
     double fsum = 0.0;
     long long mn = LLONG_MAX, mx = LLONG_MIN;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    auto row = [&](int64_t i, PL x, VT v) {
         bool keep = true;
         if constexpr (HAS_PRED) {
-            const PL x = reinterpret_cast<const PL*>(pcol)[i];
             keep = ((x >= plo) & (x <= phi)) != (pi.invert != 0);
             if (pnull) keep = keep && !((pnull[i >> 6] >> (i & 63)) & 1ull);
         }
         if (mask) keep = keep && mask[i] != 0;
         if (vnull) keep = keep && !((vnull[i >> 6] >> (i & 63)) & 1ull);
-        if (!keep) continue;
-        const VT v = vals[i];
+        if (!keep) return;
         ++cnt;
         if constexpr (VFLOAT) fsum += static_cast<double>(v);
         else isum += static_cast<unsigned long long>(static_cast<long long>(v));
         const long long e = sc_enc(v);
         mn = min(mn, e);
         mx = max(mx, e);
+    };
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    // Four rows per thread and step, all loads issued before any is used, so that enough bytes are in flight per SM
+    // to cover the memory latency at full bandwidth.
+    constexpr int U = 4;
+    for (; i + (U - 1) * stride < n; i += U * stride) {
+        PL x[U];
+        VT v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            x[u] = HAS_PRED ? __ldcs(reinterpret_cast<const PL*>(pcol) + i + u * stride) : PL{};
+            v[u] = __ldcs(vals + i + u * stride);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) row(i + u * stride, x[u], v[u]);
     }
+    for (; i < n; i += stride) row(i, HAS_PRED ? reinterpret_cast<const PL*>(pcol)[i] : PL{}, vals[i]);
     // warp, then block reduce
     for (int d = 16; d > 0; d >>= 1) {
         cnt += __shfl_down_sync(0xffffffffu, cnt, d);
@@ -107,8 +121,16 @@ template <typename VT, typename PT>
 static void scalar_launch(const void* vals, const uint64_t* vnull, int64_t n, const void* pcol, const uint64_t* pnull,
                           const PredInterval& pi, const int8_t* mask, ScalarState* st, cudaStream_t s) {
     const DeviceInfo& di = device_info();
-    const unsigned grid = static_cast<unsigned>(
-        std::max<int64_t>(1, std::min<int64_t>((n + kScThreads - 1) / kScThreads, int64_t(di.sm_count) * 8)));
+    // One wave: as many blocks as are resident on every SM at once.
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, scalar_kernel<VT, PT>, kScThreads, 0) != cudaSuccess || b < 1)
+            b = 4;
+        per_sm = b;
+    }
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
+        1, std::min<int64_t>((n + kScThreads - 1) / kScThreads, int64_t(di.sm_count) * per_sm)));
     scalar_kernel<VT, PT><<<grid, kScThreads, 0, s>>>(static_cast<const VT*>(vals), vnull, n,
                                                        static_cast<const PT*>(pcol), pnull, pi, mask, st);
     note_launch();

@@ -137,6 +137,30 @@ def test_string_groupby_near_keys_are_distinct():
         assert got[k]["count"] == 50 and got[k]["sum"] == int(idx.sum()) and got[k]["min"] == i
 
 
+def test_string_groupby_long_keys_use_the_arena():
+    """Keys of 5..195 bytes (inline words and arena words), many sharing long prefixes, against the oracle."""
+    rng = np.random.default_rng(8)
+    base = [b"p" * int(L) + b"%05d" % i for i, L in enumerate(rng.integers(0, 190, 3000))]
+    n = 200_000
+    keys = [base[i] for i in rng.integers(0, len(base), n)]
+    chars, ends = oracle.pack_strings(keys)
+    vals = rng.integers(-100, 100, n).astype(np.int32)
+    tab = StringGroupByTable(AGGS, np.int32, 4096, max_key_bytes=4096 * 200)
+    tab.process(GPUString(_dev(chars), _dev(ends)), _dev(vals))
+    _check_against_oracle(tab, chars, ends, vals, None, None, None, np.int32)
+
+
+def test_string_groupby_unaligned_character_buffer():
+    """A character buffer that starts at an odd address (a slice of a larger buffer)."""
+    keys = [b"alpha", b"beta", b"", b"gamma-delta-epsilon-zeta-eta", b"beta", b"alpha"] * 1000
+    chars, ends = oracle.pack_strings(keys)
+    dpad = _dev(np.concatenate([np.zeros(3, dtype=np.uint8), chars]))
+    vals = np.arange(len(keys), dtype=np.int32)
+    tab = StringGroupByTable(AGGS, np.int32, 16)
+    tab.process(GPUString(dpad[3:], _dev(ends)), _dev(vals))
+    _check_against_oracle(tab, chars, ends, vals, None, None, None, np.int32)
+
+
 def test_string_groupby_count_rows_without_values():
     keys = ["x", "y", None, "x", None, "z", "x"]
     chars, ends = oracle.pack_strings(keys)
@@ -154,9 +178,12 @@ def test_string_groupby_table_full_and_arena_full():
     with pytest.raises(QueryEngineError) as e:
         tab.process(GPUString(_dev(chars), _dev(ends)), _dev(vals))
     assert e.value.code == GPU_HASH_TABLE_FULL
+    # keys longer than the 24 bytes a slot keeps inline need the arena: 64 bytes of it hold four 16-byte tails
+    long_keys = [b"%040d" % i for i in range(10)]
+    lc, le = oracle.pack_strings(long_keys)
     tab2 = StringGroupByTable(["sum"], np.int32, 2000, max_key_bytes=64)
     with pytest.raises(QueryEngineError) as e:
-        tab2.process(GPUString(_dev(chars), _dev(ends)), _dev(vals))
+        tab2.process(GPUString(_dev(lc), _dev(le)), _dev(np.ones(10, dtype=np.int32)))
     assert e.value.code == GPU_HASH_TABLE_FULL
     # the same keys fit a table sized for them
     tab3 = StringGroupByTable(["sum"], np.int32, 1000)
