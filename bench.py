@@ -18,7 +18,8 @@ On one GPU the same line also carries the other configurations, each measured af
 composite keys), `batched` (4096 instances in one CUDA graph against the plain path looped in C), `served`
 (continuous batching over 2^30 resident rows at four Poisson rates), and the operators next to the path:
 `scalar_256m` (the filtered workload's WHERE and values without GROUP BY), `string_32m` (GROUP BY over 2^25 string
-keys) and `order_by_groups` (ORDER BY SUM DESC of the string GROUP BY's groups); --headline-only skips them.
+keys), `order_by_groups` (ORDER BY SUM DESC of the string GROUP BY's groups) and `compressed_keys_256m` (the
+headline workload with its keys as an AAFL-compressed block); --headline-only skips them.
 
 --impl reference times the reference's CPU-side GROUP BY (the hash-map aggregation its tests check against,
 restated in oracle/) on all host threads over the same workload.
@@ -68,10 +69,10 @@ def parse_args():
                     help="skip the plain, composite, batched and served sub-workloads of the default run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="filtered",
-                    choices=["filtered", "batched", "served", "plain", "composite", "scalar", "string"])
+                    choices=["filtered", "batched", "served", "plain", "composite", "scalar", "string", "compressed"])
     ap.add_argument("--composite-rows", type=int, default=1 << 27)
     ap.add_argument("--no-oracle", action="store_true",
-                    help="plain / composite / scalar / string on their own: skip the oracle leg (profiling runs)")
+                    help="plain / composite / scalar / string / compressed on their own: skip the oracle leg")
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
     ap.add_argument("--plain-sample", type=int, default=0,
                     help="batched / served: queries of the one-by-one plain-path comparison (0 = all / 24)")
@@ -392,6 +393,8 @@ def run_ours(args):
         subs["scalar_256m"] = scalar_measure(args, dev)
         torch.cuda.empty_cache()
         subs["string_32m"], subs["order_by_groups"] = string_and_order_measure(args, dev)
+        torch.cuda.empty_cache()
+        subs["compressed_keys_256m"] = compressed_measure(args, dev)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -695,6 +698,77 @@ def string_and_order_measure(args, dev) -> tuple:
                              "sample": f"all {g} rows, stable sort, {ob_cpu * 1e3:.1f} ms"}
     o_out["parity"] = {"checked_against": "oracle stable ORDER BY of the same column", "exact": same, "parity": same}
     return s_out, o_out
+
+
+AAFL_WORKLOAD = ("filtered-groupby-256M-aafl-keys: the filtered workload (2^28 rows, f32 pred p<0.5, f32 lognormal(2,1) "
+                 "values, SUM+AVG) with int64 Zipf(1.1) keys as ranks 1..1M stored as an AAFL-compressed block "
+                 "(20 bits per key); keys unpacked inside the aggregation pass")
+
+
+def compressed_measure(args, dev) -> dict:
+    import torch
+
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import AaflBlock, FilterConditions, GroupByTable, make_pred, process_aafl
+    n = args.rows
+    k = dg.zipf_i64(SEED, 1, n, N_DISTINCT, 1.1, map_keys=False)
+    p = dg.uniform_f32(SEED, 0, n)
+    v = dg.lognormal_f32(SEED, 2, n, 2.0, 1.0)
+    dk, dp, dv = (torch.from_numpy(x).to(dev) for x in (k, p, v))
+    blk = AaflBlock.compress(dk, 1, N_DISTINCT)
+    block_bytes = blk.elements * 8
+    pred = make_pred(dp, FilterConditions.less, 0.5, np.float32)
+    t = GroupByTable(["sum", "avg"], np.int64, np.float32, 1 << 20)
+    agg = {"aafl": [], "plain": []}
+
+    def step(kind):
+        t.reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if kind == "aafl":
+            process_aafl(t, blk, dv, pred, sync=False)
+        else:
+            t.process([dk], dv, n, pred=pred, sync=False)
+        e1.record()
+        t.results(["sum", "avg"])
+        agg[kind].append((e0, e1))
+
+    ms = statistics.median(_event_steps(lambda: step("aafl"), args.steps, args.warmup))
+    t.check()
+    kms = statistics.median(x.elapsed_time(z) for x, z in agg["aafl"][args.warmup:])
+    g = t.results_numpy(["sum", "avg"])
+    _event_steps(lambda: step("plain"), args.steps, args.warmup)
+    pkms = statistics.median(x.elapsed_time(z) for x, z in agg["plain"][args.warmup:])
+    alg = n * 8 + block_bytes
+    peak, peak_kind = measured_peak()
+    out = {"workload": AAFL_WORKLOAD, "metric": "filtered GROUP BY rows/s", "unit": "rows/s",
+           "value": n / (ms / 1e3), "ms_per_step": ms, "block_bytes": block_bytes,
+           "key_bytes_per_row": block_bytes / n,
+           "step": "reset + aggregation pass unpacking the key block + spill pass + GetResults",
+           "roofline": {"bound": "hbm", "achieved": alg / (kms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": alg / (kms / 1e3) / 1e9 / peak, "kernel_ms": kms,
+                        "kernel": "gb_fast_kernel (keys unpacked in the consumer warps) + gb_fspill_kernel",
+                        "algorithmic_bytes_per_launch": alg, "peak_kind": peak_kind},
+           "plain_keys_kernel_ms": pkms}
+    del dk, dp, dv, pred, blk
+    if getattr(args, "no_oracle", False):
+        return out
+    # cpu_baseline leg: the oracle over every row of the plain columns; its result checks the GPU's
+    import oracle
+    r = oracle.groupby(k, v, pred=(p, FilterConditions.less, 0.5, np.float32, None), threads=0)
+    order = np.argsort(g["keys"][0], kind="stable")
+    ok = g["n_groups"] == r["count"] and bool(np.array_equal(g["keys"][0][order], r["keys"][0]))
+    err = 0.0
+    if ok:
+        for a in ("sum", "avg"):
+            e = np.abs(g[a][order].astype(np.float64) - r[a]) / np.maximum(np.abs(r[a]), 1e-30)
+            err = max(err, float(e.max()))
+    out["cpu_baseline"] = {"value": n / r["seconds"], "unit": "rows/s", "cores": r["threads"], "kind": "port",
+                           "sample": f"all {n} rows (plain columns), {r['threads']} threads, {r['seconds']:.2f} s"}
+    out["parity"] = {"checked_against": "oracle over every row of the plain columns", "groups": int(r["count"]),
+                     "keys_exact": bool(ok), "max_rel_err": err, "parity": bool(ok and err <= FLOAT_RTOL)}
+    return out
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -1088,11 +1162,11 @@ def run_sub(args, fn):
 
 def main():
     args = parse_args()
-    if args.workload in ("plain", "composite", "scalar", "string"):
+    if args.workload in ("plain", "composite", "scalar", "string", "compressed"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the headline workload"}))
             return
-        fn = {"plain": c0_measure, "composite": c2_measure, "scalar": scalar_measure,
+        fn = {"plain": c0_measure, "composite": c2_measure, "scalar": scalar_measure, "compressed": compressed_measure,
               "string": lambda a, d: dict(zip(("string_32m", "order_by_groups"), string_and_order_measure(a, d)))}
         run_sub(args, fn[args.workload])
         return

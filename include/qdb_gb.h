@@ -162,6 +162,45 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
 int32_t qdb_gb_process_host(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls,
                             const void* vals, const uint64_t* val_nulls, int64_t n, const qdb_pred* pred,
                             const int8_t* mask, int64_t chunk_rows, void* stream);
+/* ---- compressed column blocks: AAFL (qikkDB/Compression/GPUCompression.cu:25-148, :474-522; the block format
+ *      of CompressionGPU::compressDataAAFL and the bit packing of feathergpu fl/aafl.cuh, fl/afl.cuh) ----
+ * A block as the reference stores it, on the device: int64 rows, int64 elements (its length in elements of the
+ * type), int64 blocks (= ceil(rows / 32)), uint64 position[blocks], uint8 bit_length[blocks], then the packed words.
+ * Rows come in groups of 32 W (W = bits of the type): row d is lane d % 32, value (d % 32W) / 32 of its group, and
+ * takes bit_length[g] bits of the lane's stream (words position[g] + lane + 32 k), to which the offset (the block's
+ * min, or 0 when max - min does not fit the type) is added back.  FLOAT blocks are their int32 bit patterns (the
+ * reference compresses only single-sign float blocks).  min_bits / max_bits carry the block's min and max (the
+ * BlockBase statistics the dispatcher passes to Decompress) as the type's bit pattern in the low bytes. */
+typedef struct qdb_aafl_col {
+    const void* data;    /* device: the compressed block */
+    int32_t type;        /* QDB_INT32, QDB_INT64 or QDB_FLOAT */
+    int32_t reserved;
+    int64_t rows;        /* the header's three counts */
+    int64_t elements;
+    int64_t blocks;
+    int64_t min_bits;
+    int64_t max_bits;
+} qdb_aafl_col;
+/* CompressionGPU::decompressDataAAFLOnDevice: writes the block's rows to `out` (device, rows elements of the
+ * type).  A block whose words do not match its header latches nothing here: the call returns QDB_ERR_INVALID after
+ * synchronising `stream` when a position or bit length points outside the packed words. */
+int32_t qdb_aafl_decompress(const qdb_aafl_col* col, void* out, void* stream);
+/* CompressionGPU::compressDataAAFL (GPUCompression.cu:25-148, on a device column): compresses `rows` values of
+ * `type` at `in` with the block's min and max (bit patterns as in qdb_aafl_col) into a newly allocated block
+ * (*out_block, *out_elements elements of the type; release with qdb_free), groups placed in row order.  A block that
+ * would not be smaller than the column (or a FLOAT column whose values mix signs) stays plain: *out_block is NULL.
+ * Synchronises `stream`. */
+int32_t qdb_aafl_compress(int32_t type, const void* in, int64_t rows, int64_t min_bits, int64_t max_bits,
+                          void** out_block, int64_t* out_elements, void* stream);
+/* ProcessBlock of a single-key table whose key column is an AAFL block (the dispatcher's decompress-then-aggregate,
+ * GpuSqlDispatcherVMFunctions.h:228-250, fused): in the fast pass the consumer warps unpack their rows' keys from the
+ * packed words into shared memory, so the key column costs its compressed bytes of HBM traffic.  `vals` (plain,
+ * val_type's column of rows values) and `pred` (plain columns) as in qdb_gb_process; no NULL masks.  When the fast
+ * pass does not apply (a table placed QDB_PLACE_GLOBAL, fewer than 2048 rows, unaligned columns) the keys are
+ * decompressed into a temporary column first.  The key type must be the table's.  Asynchronous like qdb_gb_process;
+ * a malformed block latches QDB_ERR_INVALID for qdb_gb_check. */
+int32_t qdb_gb_process_aafl(qdb_gb* gb, const qdb_aafl_col* keys, const void* vals, const qdb_pred* pred,
+                            void* stream);
 /* Synchronises `stream`, returns and clears the latched kernel status (QDB_OK or QDB_HASH_TABLE_FULL). */
 int32_t qdb_gb_check(qdb_gb* gb, void* stream);
 /* ProcessBlock followed by the Swap check: the synchronous form the reference exposes. */

@@ -51,6 +51,9 @@ def lib() -> C.CDLL:
         L.oracle_prefix_sum.argtypes = [P, I64, P]
         L.oracle_reference_filter_inputs.argtypes = [I32, I32, I64, P, P]
         L.oracle_order_by.argtypes = [I32, P, P, P, P, I64, P]
+        L.oracle_aafl_compress.restype = I64
+        L.oracle_aafl_compress.argtypes = [I32, P, I64, P, P, P, I64]
+        L.oracle_aafl_decompress.argtypes = [I32, P, P, P, P]
         L.oracle_string_ids.restype = I64
         L.oracle_string_ids.argtypes = [P, P, P, I64, P]
         _lib = L
@@ -145,6 +148,37 @@ def groupby_string(chars, ends, vals=None, key_nulls=None, val_nulls=None, mask=
     for j in range(r["count"]):
         key = None if r["key_nulls"][0][j] else string_at(chars, ends, int(r["keys"][0][j]))
         out[key] = {f: r[f][j] for f in ("cnt", "sum", "min", "max", "avg", "val_null")}
+    return out
+
+
+def aafl_compress(values: np.ndarray, vmin=None, vmax=None):
+    """AAFL block of a column (int32, int64 or float32) with its min and max (default: the column's own), or None
+    when the block stays plain.  Returns the block as an array of the column's dtype."""
+    v = np.ascontiguousarray(values)
+    dt = v.dtype
+    mn = np.array([v.min() if vmin is None else vmin], dtype=dt)
+    mx = np.array([v.max() if vmax is None else vmax], dtype=dt)
+    out = np.zeros(len(v) + 64, dtype=dt)
+    r = lib().oracle_aafl_compress(NP_CODE[dt], _p(v), len(v), _p(mn), _p(mx), _p(out), len(out))
+    if r <= 0:
+        return None
+    return out[:r].copy()
+
+
+def aafl_header(block: np.ndarray) -> tuple:
+    """(rows, elements, blocks) of an AAFL block."""
+    h = np.frombuffer(np.ascontiguousarray(block).tobytes()[:24], dtype=np.int64)
+    return int(h[0]), int(h[1]), int(h[2])
+
+
+def aafl_decompress(block: np.ndarray, vmin, vmax) -> np.ndarray:
+    b = np.ascontiguousarray(block)
+    dt = b.dtype
+    rows = aafl_header(b)[0]
+    out = np.empty(rows, dtype=dt)
+    mn = np.array([vmin], dtype=dt)
+    mx = np.array([vmax], dtype=dt)
+    lib().oracle_aafl_decompress(NP_CODE[dt], _p(b), _p(mn), _p(mx), _p(out))
     return out
 
 

@@ -30,6 +30,7 @@
 #include <random>
 #include <string_view>
 #include <thread>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -439,6 +440,173 @@ int64_t oracle_string_ids(const char* chars, const int64_t* ends, const uint64_t
         out[i] = first.emplace(s, i).first->second;
     }
     return static_cast<int64_t>(first.size());
+}
+
+// ---- AAFL compressed blocks (the block format of qikkDB/Compression/GPUCompression.cu:25-148 with the bit
+// packing of feathergpu fl/aafl.cuh:5-58 and fl/afl.cuh:6-77), restated for 32- and 64-bit integers and for
+// floats of one sign (compressed as their int32 bit patterns, GPUCompression.cu:197-225).
+// A block of T elements: int64 rows, int64 elements (the block's length in T), int64 blocks (= ceil(rows / 32));
+// uint64 position[blocks]; uint8 bit_length[blocks]; then the packed words (T).  Rows are packed in groups of
+// 32 W (W = bits of T): row d of group g is lane d % 32, index i = (d % 32W) / 32; lane l's values i = 0, 1, ...
+// occupy bits [i b, (i + 1) b) of the lane's bit stream, word k of which is words[position[g] + l + 32 k]
+// (least significant bit first), b = bit_length[g] = significant bits of the group's largest (value - offset).
+// The compressor here places the groups' words in group order (the reference takes them in the order its warps
+// finish); any placement decodes the same.
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+T aafl_offset(T mn, T mx) {
+    // offset = min, or 0 when max - min does not fit T; -min wraps as two's complement does for lowest(T)
+    using U = typename std::make_unsigned<T>::type;
+    T off = mn;
+    if (mn < 0 && mx > 0) {
+        const T neg = static_cast<T>(U(0) - static_cast<U>(mn));
+        if (std::numeric_limits<T>::max() - mx < neg) off = 0;
+    }
+    return off;
+}
+
+template <typename T>
+int64_t aafl_compress_t(const T* v, int64_t n, T mn, T mx, T* out, int64_t cap) {
+    using U = typename std::make_unsigned<T>::type;
+    constexpr int W = sizeof(T) * 8;
+    const T off = aafl_offset(mn, mx);
+    const int64_t blocks = (n + 31) / 32;
+    const int64_t groups = (n + 32 * W - 1) / (32 * W);
+    std::vector<uint64_t> pos(static_cast<size_t>(blocks), 0);
+    std::vector<uint8_t> bl(static_cast<size_t>(blocks), 0);
+    std::vector<U> words;
+    for (int64_t g = 0; g < groups; ++g) {
+        const int64_t d0 = g * 32 * W;
+        U mxv = 0;
+        for (int64_t d = d0; d < std::min<int64_t>(n, d0 + 32 * W); ++d) mxv = std::max<U>(mxv, static_cast<U>(static_cast<U>(v[d]) - static_cast<U>(off)));
+        int b = 0;
+        while (b < W && (mxv >> b) != 0) ++b;
+        const int64_t rem = n - d0;
+        int64_t space = static_cast<int64_t>(b) * 32;
+        if (rem < 32 * W) space = ((((rem + W - 1) / W) * b + 31) / 32) * 32;  // GPUCompression's last-group size
+        pos[static_cast<size_t>(g)] = words.size();
+        bl[static_cast<size_t>(g)] = static_cast<uint8_t>(b);
+        const size_t base = words.size();
+        words.resize(base + static_cast<size_t>(space), 0);
+        if (b == 0) continue;
+        for (int l = 0; l < 32; ++l) {
+            for (int i = 0; i < W; ++i) {
+                const int64_t d = d0 + l + 32 * i;
+                if (d >= n) break;
+                const U x = static_cast<U>(static_cast<U>(v[d]) - static_cast<U>(off));
+                const int64_t o = static_cast<int64_t>(i) * b;
+                const int64_t k = o / W;
+                const int p = static_cast<int>(o % W);
+                words[base + static_cast<size_t>(l + 32 * k)] |= static_cast<U>(x << p);
+                if (p + b > W) words[base + static_cast<size_t>(l + 32 * (k + 1))] |= static_cast<U>(x >> (W - p));
+            }
+        }
+    }
+    const int64_t data_bytes = static_cast<int64_t>(words.size()) * static_cast<int64_t>(sizeof(T));
+    const int64_t total = data_bytes + std::max<int64_t>(8 * blocks, sizeof(T)) + std::max<int64_t>(blocks, sizeof(T)) + 24;
+    const int64_t elems = (total + static_cast<int64_t>(sizeof(T)) - 1) / static_cast<int64_t>(sizeof(T));
+    if (elems >= n) return 0;  // compression does not pay: the block stays plain
+    if (elems > cap) return -elems;
+    char* o = reinterpret_cast<char*>(out);
+    std::memset(o, 0, static_cast<size_t>(elems) * sizeof(T));
+    const int64_t hdr[3] = {n, elems, blocks};
+    std::memcpy(o, hdr, 24);
+    std::memcpy(o + 24, pos.data(), static_cast<size_t>(blocks) * 8);
+    std::memcpy(o + 24 + 8 * blocks, bl.data(), static_cast<size_t>(blocks));
+    std::memcpy(o + 24 + 9 * blocks, words.data(), static_cast<size_t>(data_bytes));
+    return elems;
+}
+
+template <typename T>
+void aafl_decompress_t(const T* c, T mn, T mx, T* out) {
+    using U = typename std::make_unsigned<T>::type;
+    constexpr int W = sizeof(T) * 8;
+    const char* b = reinterpret_cast<const char*>(c);
+    int64_t hdr[3];
+    std::memcpy(hdr, b, 24);
+    const int64_t n = hdr[0], blocks = hdr[2];
+    const T off = aafl_offset(mn, mx);
+    const int64_t groups = (n + 32 * W - 1) / (32 * W);
+    for (int64_t g = 0; g < groups; ++g) {
+        uint64_t base;
+        std::memcpy(&base, b + 24 + 8 * g, 8);
+        const int bits = static_cast<uint8_t>(b[24 + 8 * blocks + g]);
+        const char* words = b + 24 + 9 * blocks;
+        auto word = [&](int64_t idx) {
+            U w;
+            std::memcpy(&w, words + idx * static_cast<int64_t>(sizeof(T)), sizeof(T));
+            return w;
+        };
+        for (int l = 0; l < 32; ++l) {
+            for (int i = 0; i < W; ++i) {
+                const int64_t d = g * 32 * W + l + 32 * i;
+                if (d >= n) break;
+                U x = 0;
+                if (bits) {
+                    const int64_t o = static_cast<int64_t>(i) * bits;
+                    const int64_t k = o / W;
+                    const int p = static_cast<int>(o % W);
+                    x = static_cast<U>(word(static_cast<int64_t>(base) + l + 32 * k) >> p);
+                    if (p + bits > W) x |= static_cast<U>(word(static_cast<int64_t>(base) + l + 32 * (k + 1)) << (W - p));
+                    if (bits < W) x &= static_cast<U>((U(1) << bits) - 1);
+                }
+                out[d] = static_cast<T>(static_cast<U>(x + static_cast<U>(off)));
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// Compresses n values of type (T_INT32, T_INT64, T_FLOAT) with the block's min and max (host values of the type).
+// Returns the block's length in elements (written to out), 0 when the block stays plain (compression would not
+// shrink it, or a float block mixes signs), or -needed when cap elements are too few.
+int64_t oracle_aafl_compress(int32_t type, const void* in, int64_t n, const void* mn, const void* mx, void* out,
+                             int64_t cap) {
+    switch (type) {
+        case T_INT32: return aafl_compress_t(static_cast<const int32_t*>(in), n, *static_cast<const int32_t*>(mn),
+                                             *static_cast<const int32_t*>(mx), static_cast<int32_t*>(out), cap);
+        case T_INT64: return aafl_compress_t(static_cast<const int64_t*>(in), n, *static_cast<const int64_t*>(mn),
+                                             *static_cast<const int64_t*>(mx), static_cast<int64_t*>(out), cap);
+        case T_FLOAT: {
+            const float fmn = *static_cast<const float*>(mn), fmx = *static_cast<const float*>(mx);
+            if (!((fmn >= 0 && fmx >= 0) || (fmn <= 0 && fmx <= 0))) return 0;
+            int32_t a, b;
+            std::memcpy(&a, &fmn, 4);
+            std::memcpy(&b, &fmx, 4);
+            if (a > b) std::swap(a, b);
+            return aafl_compress_t(static_cast<const int32_t*>(in), n, a, b, static_cast<int32_t*>(out), cap);
+        }
+        default: return 0;
+    }
+}
+
+// Decompresses a block (its header gives the row count) into out.
+void oracle_aafl_decompress(int32_t type, const void* in, const void* mn, const void* mx, void* out) {
+    switch (type) {
+        case T_INT32:
+            aafl_decompress_t(static_cast<const int32_t*>(in), *static_cast<const int32_t*>(mn),
+                              *static_cast<const int32_t*>(mx), static_cast<int32_t*>(out));
+            break;
+        case T_INT64:
+            aafl_decompress_t(static_cast<const int64_t*>(in), *static_cast<const int64_t*>(mn),
+                              *static_cast<const int64_t*>(mx), static_cast<int64_t*>(out));
+            break;
+        case T_FLOAT: {
+            int32_t a, b;
+            std::memcpy(&a, mn, 4);
+            std::memcpy(&b, mx, 4);
+            if (a > b) std::swap(a, b);
+            aafl_decompress_t(static_cast<const int32_t*>(in), a, b, static_cast<int32_t*>(out));
+            break;
+        }
+        default: break;
+    }
 }
 
 int64_t oracle_indexes(const int8_t* mask, int64_t n, int32_t* out) {

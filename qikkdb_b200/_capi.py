@@ -51,6 +51,19 @@ class qdb_pred(C.Structure):
     ]
 
 
+class qdb_aafl_col(C.Structure):
+    _fields_ = [
+        ("data", C.c_void_p),
+        ("type", C.c_int32),
+        ("reserved", C.c_int32),
+        ("rows", C.c_int64),
+        ("elements", C.c_int64),
+        ("blocks", C.c_int64),
+        ("min_bits", C.c_int64),
+        ("max_bits", C.c_int64),
+    ]
+
+
 class qdb_gb_query(C.Structure):
     _fields_ = [
         ("agg_mask", C.c_int32),
@@ -172,6 +185,9 @@ SIGNATURES = [
     ("qdb_gbs_process", I32, [P, P, P, P, P, P, P, I64, P]),
     ("qdb_gbs_check", I32, [P, P]),
     ("qdb_gbs_results", I32, [P, I32, P, PP, PP, PP, PP, PP, C.POINTER(I64), P]),
+    ("qdb_aafl_decompress", I32, [C.POINTER(qdb_aafl_col), P, P]),
+    ("qdb_aafl_compress", I32, [I32, P, I64, I64, I64, PP, C.POINTER(I64), P]),
+    ("qdb_gb_process_aafl", I32, [P, C.POINTER(qdb_aafl_col), P, C.POINTER(qdb_pred), P]),
     ("qdb_pred_block_may_pass", I32, [C.POINTER(qdb_pred), P, P, C.POINTER(I32)]),
     ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
     ("qdb_server_destroy", I32, [P]),

@@ -7,6 +7,7 @@
 #include <mutex>
 #include <vector>
 
+#include "aafl.cuh"
 #include "groupby_fast.cuh"
 
 namespace qdb {
@@ -607,13 +608,16 @@ int32_t qdb_gb_reset(qdb_gb* gb, void* stream) {
     return QDB_OK;
 }
 
-int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls, const void* vals,
-                       const uint64_t* val_nulls, int64_t n, const qdb_pred* pred, const int8_t* mask,
-                       void* stream) {
+// A compressed-key call (kz) that the fast pass cannot take: the caller decompresses the keys instead.
+constexpr int32_t kNotFused = -1;
+
+static int32_t process_impl(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls, const void* vals,
+                            const uint64_t* val_nulls, int64_t n, const qdb_pred* pred, const int8_t* mask,
+                            void* stream, const AaflView* kz) {
     if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_process: null table");
     if (n < 0) return fail(QDB_ERR_INVALID, "qdb_gb_process: negative row count");
     if (n == 0) return QDB_OK;
-    if (!key_cols || !key_cols[0] || (gb->n_key_cols == 2 && !key_cols[1]))
+    if (!kz && (!key_cols || !key_cols[0] || (gb->n_key_cols == 2 && !key_cols[1])))
         return fail(QDB_ERR_INVALID, "qdb_gb_process: missing key column");
     if (gb->val_type != 0 && !vals) return fail(QDB_ERR_INVALID, "qdb_gb_process: missing value column");
     int32_t ptype = 0;
@@ -637,8 +641,16 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     }
 
     AggArgs a;
-    a.key0 = key_cols[0];
-    a.key1 = gb->n_key_cols == 2 ? key_cols[1] : nullptr;
+    a.key0 = kz ? nullptr : key_cols[0];
+    a.key1 = (!kz && gb->n_key_cols == 2) ? key_cols[1] : nullptr;
+    if (kz) {
+        a.kz = 1;
+        a.kz_words = kz->words;
+        a.kz_pos = kz->pos;
+        a.kz_bits = kz->bits;
+        a.kz_off = kz->off;
+        a.kz_len = kz->words_len;
+    }
     a.knull0 = kn0;
     a.knull1 = kn1;
     a.vals = gb->val_type ? vals : nullptr;
@@ -661,12 +673,13 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     a.capacity = static_cast<unsigned long long>(gb->capacity);
     const bool nulls = a.knull0 || a.knull1 || a.vnull || a.pnull;
     if (!nulls && !mask && gb->placement != QDB_PLACE_GLOBAL && n >= kFastT && env_int("QDB_AGG_FAST", 1) != 0 &&
-        aligned16(a.key0) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
+        (kz || aligned16(a.key0)) && (!a.key1 || aligned16(a.key1)) && (!a.vals || aligned16(a.vals)) &&
         (!a.pcol || aligned16(a.pcol))) {
         bool used = false;
         const int32_t rc = process_fast(gb, a, pred, ptype, s, &used);
         if (rc != QDB_OK || used) return rc;
     }
+    if (kz) return kNotFused;
 
     // Tile and stage plan: stages of about 32 KB (a stage costs a fixed hand-off between the producer and
     // the consumers, so small stages cannot reach the HBM bandwidth), three of them in the ring.
@@ -823,6 +836,34 @@ int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* 
     return rc;
 }
 
+
+int32_t qdb_gb_process(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls, const void* vals,
+                       const uint64_t* val_nulls, int64_t n, const qdb_pred* pred, const int8_t* mask,
+                       void* stream) {
+    return process_impl(gb, key_cols, key_nulls, vals, val_nulls, n, pred, mask, stream, nullptr);
+}
+
+int32_t qdb_gb_process_aafl(qdb_gb* gb, const qdb_aafl_col* keys, const void* vals, const qdb_pred* pred,
+                            void* stream) {
+    if (!gb || !keys) return fail(QDB_ERR_INVALID, "qdb_gb_process_aafl: null argument");
+    if (gb->n_key_cols != 1 || keys->type != gb->key_type)
+        return fail(QDB_ERR_INVALID, "qdb_gb_process_aafl: the block's type must be the single key type of the table");
+    cudaStream_t s = as_stream(stream);
+    AaflView v;
+    int32_t rc = aafl_view(keys, &v, s);
+    if (rc != QDB_OK || v.rows == 0) return rc;
+    rc = process_impl(gb, nullptr, nullptr, vals, nullptr, v.rows, pred, nullptr, stream, &v);
+    if (rc == kNotFused) {
+        void* col = nullptr;
+        rc = dev_alloc(&col, static_cast<size_t>(v.rows) * v.word_bytes, s);
+        if (rc == QDB_OK) rc = qdb_aafl_decompress(keys, col, stream);
+        const void* kc[1] = {col};
+        if (rc == QDB_OK) rc = process_impl(gb, kc, nullptr, vals, nullptr, v.rows, pred, nullptr, stream, nullptr);
+        dev_free(col, s);
+    }
+    dev_free(v.scratch, s);  // stream-ordered: after the pass that reads it
+    return rc;
+}
 
 int32_t qdb_gb_check(qdb_gb* gb, void* stream) {
     if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_check: null table");

@@ -111,6 +111,15 @@ struct AggArgs {
     int64_t spill2_cell = 0;
     int32_t spill2_bits = 0;
     int32_t so_spill2 = 0;            // shared-memory offset of the spill pass's second-level fill counters
+    // AAFL-compressed key column (fast pass, single key): key0 is unused; the consumer warps unpack their rows' keys
+    // from the groups' packed words (kz_words, kz_len of them; group g at kz_pos[g] with kz_bits[g] bits per value)
+    // into the ring and add kz_off back.
+    int32_t kz = 0;
+    const void* kz_words = nullptr;
+    const uint64_t* kz_pos = nullptr;
+    const uint8_t* kz_bits = nullptr;
+    uint64_t kz_off = 0;
+    int64_t kz_len = 0;
 };
 
 template <typename A, typename B>

@@ -556,6 +556,41 @@ struct FastWarp {
     }
 };
 
+// Key of row R of an AAFL-compressed key column (the block layout of qikkDB's GPUCompression.cu / feathergpu AAFL):
+// rows come in groups of 32 W (W = bits of the key type); row R is lane R % 32, value i = (R % 32W) / 32 of its group,
+// and occupies bits [i b, (i + 1) b) of the lane's stream, whose word k is words[pos[g] + lane + 32 k], least
+// significant bit first.  Lanes of a warp that hold consecutive rows read consecutive words.  A word index past the
+// packed words (a malformed block) latches QDB_ERR_INVALID and yields the offset.
+template <typename KT>
+__device__ __forceinline__ KT kz_key(const AggArgs& a, int64_t R) {
+    using WT = typename std::conditional<sizeof(KT) == 8, unsigned long long, unsigned int>::type;
+    constexpr int W = sizeof(KT) * 8;
+    const int64_t g = R / (32 * W);
+    const int i = static_cast<int>((R % (32 * W)) >> 5);
+    const int l = static_cast<int>(R & 31);
+    const int b = a.kz_bits[g];
+    WT x = 0;
+    if (b) {
+        const int o = i * b;
+        const int k = o / W;
+        const int p = o % W;
+        const int64_t i0 = static_cast<int64_t>(a.kz_pos[g]) + l + 32 * k;
+        const bool two = p + b > W;
+        if (i0 >= 0 && i0 + (two ? 32 : 0) < a.kz_len) {
+            const WT* w = static_cast<const WT*>(a.kz_words);
+            x = w[i0] >> p;
+            if (two) x |= w[i0 + 32] << (W - p);
+            if (b < W) x &= (WT(1) << b) - WT(1);
+        } else {
+            atomicExch(reinterpret_cast<int*>(&a.counters[1]), static_cast<int>(QDB_ERR_INVALID));
+        }
+    }
+    const WT v = static_cast<WT>(x + static_cast<WT>(a.kz_off));
+    KT out;
+    memcpy(&out, &v, sizeof(KT));
+    return out;
+}
+
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type (int32_t for a
 // count-only table); PT: predicate column type or NoPred; MODE: FM_* bits.
@@ -618,7 +653,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
             int64_t q = 0;
             int s = 0;
             uint32_t ph = 0;
-            uint32_t tx = static_cast<uint32_t>(kFastT) * sizeof(KT) * (COMP ? 2 : 1);
+            uint32_t tx = static_cast<uint32_t>(kFastT) * sizeof(KT) * ((COMP ? 2 : 1) - (a.kz ? 1 : 0));
             if (VALS) tx += static_cast<uint32_t>(kFastT) * sizeof(VT);
             if (HAS_PRED) tx += static_cast<uint32_t>(kFastT) * PW;
             for (; q < my_tiles; ++q) {
@@ -629,7 +664,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                 const size_t so = static_cast<size_t>(s) * kFastT;
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full_bar[s], tx);
-                bulk_g2s(ring + sl.key0 + so * sizeof(KT), static_cast<const KT*>(a.key0) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
+                if (!a.kz) bulk_g2s(ring + sl.key0 + so * sizeof(KT), static_cast<const KT*>(a.key0) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
                 if (COMP) bulk_g2s(ring + sl.key1 + so * sizeof(KT), static_cast<const KT*>(a.key1) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
                 if (VALS) bulk_g2s(ring + sl.val + so * sizeof(VT), static_cast<const VT*>(a.vals) + r0, kFastT * sizeof(VT), &full_bar[s], pol);
                 if (HAS_PRED) bulk_g2s(ring + sl.pred + so * PW, static_cast<const PL*>(a.pcol) + r0, kFastT * PW, &full_bar[s], pol);
@@ -762,7 +797,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                         act[u] = e < count;
                         const int i = HAS_PRED ? list[act[u] ? e : e0] : w0 + (act[u] ? e : e0);
                         if constexpr (COMP) kw[u] = composite_word(static_cast<int32_t>(k0p[i]), static_cast<int32_t>(k1p[i]));
-                        else kw[u] = key_word(k0p[i]);
+                        else kw[u] = key_word(a.kz ? kz_key<KT>(a, base + i) : k0p[i]);
                         if constexpr (VALS) v[u] = vp[i];
                         else v[u] = VT{};
                     }
@@ -772,6 +807,18 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                 continue;
             }
             if (!mbar_wait(&full_bar[s], ph, a.counters)) break;
+            if constexpr (!COMP) {
+                if (a.kz) {
+                    // Compressed keys: the warp unpacks its own rows' keys into the stage (no other warp reads them).
+                    KT* kd = reinterpret_cast<KT*>(ring + sl.key0) + s * kFastT;
+#pragma unroll
+                    for (int j = 0; j < kFastSeg; ++j) {
+                        const int r = warp * kFastR + 32 * j + lane;
+                        kd[r] = kz_key<KT>(a, tile * kFastT + r);
+                    }
+                    __syncwarp();
+                }
+            }
             const bool full = (q & 127) == 0 && __any_sync(0xffffffffu, table_full(a.counters));
             // The next tile of this CTA is staged too: rows left over may wait for it.
             const bool keep_going = carry && !full && q + 1 < my_tiles && tile + gridDim.x < a.full_tiles;

@@ -608,6 +608,67 @@ class StringGroupByTable:
         return out
 
 
+class AaflBlock:
+    """An AAFL-compressed column block on the device (the block format of qikkDB's CompressionGPU::compressDataAAFL:
+    header, per-group position ids and bit lengths, packed words) with the block's min and max, which the
+    decompression needs (the dispatcher passes the block statistics).  `data` is a CUDA tensor holding the block."""
+
+    def __init__(self, data: torch.Tensor, dtype, vmin, vmax):
+        self.data = data
+        self.dtype = np.dtype(dtype)
+        hdr = data.view(torch.uint8)[:24].cpu().numpy().view(np.int64)
+        self.rows, self.elements, self.blocks = int(hdr[0]), int(hdr[1]), int(hdr[2])
+        self.vmin, self.vmax = vmin, vmax
+
+    @staticmethod
+    def from_host(block: np.ndarray, vmin, vmax, device="cuda") -> "AaflBlock":
+        return AaflBlock(torch.from_numpy(np.ascontiguousarray(block)).to(device), block.dtype, vmin, vmax)
+
+    def c(self):
+        d = capi.qdb_aafl_col()
+        d.data = _ptr(self.data)
+        d.type = NP_TO_CODE[self.dtype]
+        d.rows, d.elements, d.blocks = self.rows, self.elements, self.blocks
+        raw = lambda x: int(np.array([x], dtype=self.dtype).view(np.int32 if self.dtype.itemsize == 4 else np.int64)[0])  # noqa: E731
+        d.min_bits, d.max_bits = raw(self.vmin), raw(self.vmax)
+        return d
+
+    @staticmethod
+    def compress(col: torch.Tensor, vmin=None, vmax=None, stream=None) -> Optional["AaflBlock"]:
+        """qdb_aafl_compress of a CUDA column (int32, int64 or float32) with its min and max (default: the column's
+        own); None when the block stays plain."""
+        dt = np.dtype({torch.int32: np.int32, torch.int64: np.int64, torch.float32: np.float32}[col.dtype])
+        vmin = col.min().item() if vmin is None else vmin
+        vmax = col.max().item() if vmax is None else vmax
+        bits = lambda x: int(np.array([x], dtype=dt).view(np.int32 if dt.itemsize == 4 else np.int64)[0])  # noqa: E731
+        out = C.c_void_p()
+        elems = C.c_int64()
+        capi.check(capi.lib().qdb_aafl_compress(NP_TO_CODE[dt], _ptr(col), col.numel(), bits(vmin), bits(vmax),
+                                                C.byref(out), C.byref(elems), _stream(stream)))
+        if not out.value:
+            return None
+        buf = DeviceBuffer(out.value, elems.value, dt)
+        blk = AaflBlock(buf.torch(stream), dt, vmin, vmax)
+        buf.free(stream)
+        return blk
+
+    def decompress(self, stream=None) -> torch.Tensor:
+        """qdb_aafl_decompress: the block's rows as a CUDA tensor."""
+        out = torch.empty(max(self.rows, 1), dtype=CODE_TO_TORCH[NP_TO_CODE[self.dtype]], device=self.data.device)
+        d = self.c()
+        capi.check(capi.lib().qdb_aafl_decompress(C.byref(d), _ptr(out), _stream(stream)))
+        return out[:self.rows]
+
+
+def process_aafl(table: "GroupByTable", keys: AaflBlock, values=None, pred=None, stream=None, sync: bool = True):
+    """qdb_gb_process_aafl: ProcessBlock of a single-key table whose key column is an AAFL block."""
+    d = keys.c()
+    capi.check(capi.lib().qdb_gb_process_aafl(table.handle, C.byref(d), _ptr(values),
+                                              C.byref(pred) if pred is not None else None, _stream(stream)))
+    if sync:
+        table.check(stream)
+
+
 class ScalarAggregate:
     """Scalar aggregation over a query's blocks (qdb_scalar_*): COUNT, SUM, MIN, MAX (and AVG) of one value column,
     filtered by an optional `col OP constant` predicate and mask, NULL values skipped."""

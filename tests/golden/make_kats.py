@@ -256,7 +256,26 @@ gbs("GroupByStringNullValueSum", DNT + ":1458", "sum", vk, vv, [("Apple", 12), (
 gbs("GroupByStringNullValueAvg", DNT + ":1558", "avg", vk, vv, [("Apple", 2), ("Nut", 2), ("Straw", 2), ("car0", None)])
 gbs("GroupByStringNullValueCount", DNT + ":1654", "count", vk, vv, [("Apple", 6), ("Nut", 6), ("Straw", 4), ("car0", 0)])
 
+# AAFL compressed blocks (qikkDB_test/GPUCompressionTests.cpp:27-50 fixtures, 1024-row block, assertions at the line
+# given): the first eight 32-bit words of the compressed block as the test asserts them on Linux (an 8-byte unsigned
+# long), or "plain" when the block stays uncompressed (the test then only checks that the data is unchanged).
+GCT = "qikkDB_test/GPUCompressionTests.cpp"
+compression_cases = [
+    {"name": "CompressionInt", "source": GCT + ":79", "column": "int32 i - 512",
+     "head32": [1024, 0, 398, 0, 32, 0, 0, 0]},
+    {"name": "CompressionIntLarge", "source": GCT + ":108", "column": "int32 (i - 512) * 100000000 (wrapping)",
+     "head32": "plain"},
+    {"name": "CompressionLong", "source": GCT + ":122", "column": "int64 (i - 512) * 100000",
+     "head64": [1024, 487, 32, 0, 0, 0, 0, 0]},
+    {"name": "CompressionFloatPositive", "source": GCT + ":151", "column": "float32 i / 100.0 + 10",
+     "head32": [1024, 0, 846, 0, 32, 0, 0, 0]},
+    {"name": "CompressionFloatNegative", "source": GCT + ":183", "column": "float32 -(i / 1000.0 + 10)",
+     "head32": [1024, 0, 750, 0, 32, 0, 0, 0]},
+    {"name": "CompressionFloatMixed", "source": GCT + ":229", "column": "float32 (i - 512) / 100.0",
+     "head32": "plain"},
+]
+
 with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
     json.dump({"generated_by": "tests/golden/make_kats.py", "cases": cases, "order_by_cases": order_cases,
-               "string_cases": string_cases}, f, indent=1)
+               "string_cases": string_cases, "compression_cases": compression_cases}, f, indent=1)
 print(len(cases), "cases,", len(order_cases), "ORDER BY cases,", len(string_cases), "string cases")

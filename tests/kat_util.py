@@ -80,3 +80,24 @@ def string_blocks(case):
 
 def string_expected(case):
     return {(None if e["key"] is None else e["key"].encode()): e["value"] for e in case["expected"]}
+
+
+def load_compression_kats():
+    with open(os.path.join(HERE, "golden", "reference_kats.json")) as f:
+        return json.load(f)["compression_cases"]
+
+
+def compression_column(name: str) -> np.ndarray:
+    """The 1024-row columns of qikkDB_test/GPUCompressionTests.cpp:44-52 (block size 1024)."""
+    i = np.arange(1024)
+    if name == "CompressionInt":
+        return (i - 512).astype(np.int32)
+    if name == "CompressionIntLarge":
+        return ((i - 512) * 100000000).astype(np.int64).astype(np.int32)
+    if name == "CompressionLong":
+        return ((i - 512) * 100000).astype(np.int64)
+    if name == "CompressionFloatPositive":
+        return (i / 100.0 + 10).astype(np.float32)
+    if name == "CompressionFloatNegative":
+        return -((i / 1000.0 + 10).astype(np.float32))
+    return ((i - 512) / 100.0).astype(np.float32)
