@@ -17,8 +17,9 @@ struct AaflView {
     void* scratch = nullptr;         // an aligned copy of the words, when the block's words start unaligned
 };
 
-// Checks a block's header counts and builds its view on `s` (an unaligned word region is copied to an aligned
-// scratch buffer, which the caller releases with dev_free after its last use on `s`).
-int32_t aafl_view(const qdb_aafl_col* c, AaflView* v, cudaStream_t s);
+// Checks a block's header counts and builds its view on `s`.  A word region that does not start on an `align`-byte
+// boundary (at least the word size) is copied to an aligned scratch buffer, which the caller releases with dev_free
+// after its last use on `s`.
+int32_t aafl_view(const qdb_aafl_col* c, AaflView* v, cudaStream_t s, int align = 0);
 
 }  // namespace qdb

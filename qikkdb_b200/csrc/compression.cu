@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(1024) aafl_scan_kernel(const long long* __rest
 
 }  // namespace
 
-int32_t aafl_view(const qdb_aafl_col* c, AaflView* v, cudaStream_t s) {
+int32_t aafl_view(const qdb_aafl_col* c, AaflView* v, cudaStream_t s, int align) {
     if (!c || !v || !c->data) return fail(QDB_ERR_INVALID, "AAFL block: null block");
     if (c->type != QDB_INT32 && c->type != QDB_INT64 && c->type != QDB_FLOAT)
         return fail(QDB_ERR_INVALID, "AAFL block: type must be INT32, INT64 or FLOAT");
@@ -174,7 +174,7 @@ int32_t aafl_view(const qdb_aafl_col* c, AaflView* v, cudaStream_t s) {
     v->bits = reinterpret_cast<const uint8_t*>(base + 24 + 8 * c->blocks);
     v->words_len = (c->elements * ws - meta) / ws;
     const char* words = base + meta;
-    if (reinterpret_cast<uintptr_t>(words) % ws != 0 && v->words_len > 0) {
+    if (reinterpret_cast<uintptr_t>(words) % static_cast<uintptr_t>(std::max(align, ws)) != 0 && v->words_len > 0) {
         int32_t rc = dev_alloc(&v->scratch, static_cast<size_t>(v->words_len) * ws, s);
         if (rc != QDB_OK) return rc;
         QDB_CUDA_TRY(cudaMemcpyAsync(v->scratch, words, static_cast<size_t>(v->words_len) * ws, cudaMemcpyDeviceToDevice, s));

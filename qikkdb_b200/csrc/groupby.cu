@@ -341,13 +341,16 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
     const int stage_bytes = kFastT * row_bytes;
     int NS = static_cast<int>(env_int("QDB_FAST_STAGES", stage_bytes <= 16 * 1024 ? 4 : (stage_bytes <= 40 * 1024 ? 3 : 2)));
     NS = std::min(6, std::max(2, NS));
-    const size_t ring = static_cast<size_t>(NS) * stage_bytes;
+    // Compressed keys take each stage's key slots plus 64 bytes: a group is copied from the 16-byte boundary below
+    // its first word (kzStage in groupby_fast.cuh).
+    const size_t kz_extra = a.kz ? 64 : 0;
+    const size_t ring = static_cast<size_t>(NS) * (stage_bytes + kz_extra);
     if (ring > 128 * 1024) return QDB_OK;
     // Ring columns: stage s, row i of column c at off_c + (s T + i) * size_c.
     StageLayout sl;
     int32_t off = 0;
     sl.key0 = off;
-    off += NS * kFastT * ks;
+    off += NS * (kFastT * ks + static_cast<int32_t>(kz_extra));
     if (gb->n_key_cols == 2) {
         sl.key1 = off;
         off += NS * kFastT * ks;

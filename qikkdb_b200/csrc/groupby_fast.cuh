@@ -298,6 +298,7 @@ __device__ __forceinline__ void ftab_flush(unsigned char* sm, const AggArgs& a, 
 constexpr int FM_SUM = 1;
 constexpr int FM_MM = 2;
 constexpr int FM_VALS = 4;
+constexpr int FM_KZ = 8;  // the key column is an AAFL-compressed block (single key, not DOUBLE)
 
 template <typename VT, int MODE>
 struct FastWarp {
@@ -591,6 +592,42 @@ __device__ __forceinline__ KT kz_key(const AggArgs& a, int64_t R) {
     return out;
 }
 
+// Compressed keys in the ring: stage s's key region holds the tile's groups (one of 64-bit words, two of 32-bit),
+// group gi at byte gi kzSlot<KT>() of the region, each copied from the 16-byte boundary at or below its first word:
+// the words start `lead` bytes into the slot.  kzb[4 s + 2 gi] is the group's bit length, kzb[4 s + 2 gi + 1] its lead.
+template <typename KT>
+constexpr uint32_t kzSlot() { return 32u * sizeof(KT) * 8u * sizeof(KT) + 32u; }
+template <typename KT>
+constexpr uint32_t kzStage() { return static_cast<uint32_t>(kFastT) * sizeof(KT) + 64u; }
+
+template <typename KT>
+__device__ __forceinline__ KT kz_ring(const unsigned char* keys, const uint8_t* kzb, int g, uint64_t off) {
+    using WT = typename std::conditional<sizeof(KT) == 8, unsigned long long, unsigned int>::type;
+    constexpr int W = sizeof(KT) * 8;
+    constexpr int GW = 32 * W;
+    const int s = g / kFastT;
+    const int r = g % kFastT;
+    const int gi = r / GW;
+    const int i = (r % GW) >> 5;
+    const int l = r & 31;
+    const int b = kzb[4 * s + 2 * gi];
+    WT x = 0;
+    if (b) {
+        const WT* w = reinterpret_cast<const WT*>(keys + static_cast<size_t>(s) * kzStage<KT>() + gi * kzSlot<KT>() +
+                                                  kzb[4 * s + 2 * gi + 1]) + l;
+        const int o = i * b;
+        const int k = o / W;
+        const int p = o % W;
+        x = w[32 * k] >> p;
+        if (p + b > W) x |= w[32 * (k + 1)] << (W - p);
+        if (b < W) x &= (WT(1) << b) - WT(1);
+    }
+    const WT v = static_cast<WT>(x + static_cast<WT>(off));
+    KT out;
+    memcpy(&out, &v, sizeof(KT));
+    return out;
+}
+
 // ---------------------------------------------------------------------------------------------
 // The aggregation kernel.  KT: key column type; COMP: composite (int32, int32) key; VT: value type (int32_t for a
 // count-only table); PT: predicate column type or NoPred; MODE: FM_* bits.
@@ -610,6 +647,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
     constexpr bool VFLOAT = std::is_floating_point<VT>::value;
     constexpr bool VALS = (MODE & FM_VALS) != 0;
+    constexpr bool KZ = !COMP && (MODE & FM_KZ) != 0;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
     constexpr int PW = sizeof(PL);
 
@@ -653,7 +691,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
             int64_t q = 0;
             int s = 0;
             uint32_t ph = 0;
-            uint32_t tx = static_cast<uint32_t>(kFastT) * sizeof(KT) * ((COMP ? 2 : 1) - (a.kz ? 1 : 0));
+            uint32_t tx = static_cast<uint32_t>(kFastT) * sizeof(KT) * ((COMP ? 2 : 1) - (KZ ? 1 : 0));
             if (VALS) tx += static_cast<uint32_t>(kFastT) * sizeof(VT);
             if (HAS_PRED) tx += static_cast<uint32_t>(kFastT) * PW;
             for (; q < my_tiles; ++q) {
@@ -662,9 +700,41 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                 if (q >= a.NS && !mbar_wait(&empty_bar[s], ph ^ 1u, a.counters)) break;
                 const int64_t r0 = tile * kFastT;
                 const size_t so = static_cast<size_t>(s) * kFastT;
+                // Compressed keys: the tile's groups (one of 64-bit words, two of 32-bit) arrive as their packed words,
+                // each copied from the 16-byte boundary at or below its first word through the 16-byte chunk that holds
+                // its last (a chunk that holds a byte of the block lies in a page the block uses).
+                constexpr int KZ_GW = 32 * static_cast<int>(sizeof(KT)) * 8;
+                constexpr int KZ_NG = COMP ? 1 : kFastT / KZ_GW;
+                uint32_t kz_bytes[2] = {0u, 0u};
+                uint64_t kz_src[2] = {0ull, 0ull};
+                if constexpr (KZ) {
+                    uint8_t* kzb = reinterpret_cast<uint8_t*>(sm + a.so_bar + 96) + 4 * s;
+#pragma unroll
+                    for (int gi = 0; gi < KZ_NG; ++gi) {
+                        const int64_t g = tile * KZ_NG + gi;
+                        int b = a.kz_bits[g];
+                        const uint64_t pos = a.kz_pos[g];
+                        const uint64_t words = 32ull * static_cast<uint64_t>(b);
+                        if (b > static_cast<int>(sizeof(KT)) * 8 || pos + words > static_cast<uint64_t>(a.kz_len)) {
+                            if (b) atomicExch(reinterpret_cast<int*>(&a.counters[1]), static_cast<int>(QDB_ERR_INVALID));
+                            b = 0;
+                        }
+                        const uint64_t src = reinterpret_cast<uint64_t>(a.kz_words) + pos * sizeof(KT);
+                        const uint32_t lead = static_cast<uint32_t>(src & 15u);
+                        kzb[2 * gi] = static_cast<uint8_t>(b);
+                        kzb[2 * gi + 1] = static_cast<uint8_t>(lead);
+                        kz_bytes[gi] = b ? ((lead + static_cast<uint32_t>(words * sizeof(KT)) + 15u) & ~15u) : 0u;
+                        kz_src[gi] = src - lead;
+                    }
+                }
                 fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&full_bar[s], tx);
-                if (!a.kz) bulk_g2s(ring + sl.key0 + so * sizeof(KT), static_cast<const KT*>(a.key0) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
+                mbar_arrive_expect_tx(&full_bar[s], tx + kz_bytes[0] + kz_bytes[1]);
+#pragma unroll
+                for (int gi = 0; gi < KZ_NG; ++gi)
+                    if (kz_bytes[gi])
+                        bulk_g2s(ring + sl.key0 + static_cast<size_t>(s) * kzStage<KT>() + gi * kzSlot<KT>(),
+                                 reinterpret_cast<const void*>(kz_src[gi]), kz_bytes[gi], &full_bar[s], pol);
+                if constexpr (!KZ) bulk_g2s(ring + sl.key0 + so * sizeof(KT), static_cast<const KT*>(a.key0) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
                 if (COMP) bulk_g2s(ring + sl.key1 + so * sizeof(KT), static_cast<const KT*>(a.key1) + r0, kFastT * sizeof(KT), &full_bar[s], pol);
                 if (VALS) bulk_g2s(ring + sl.val + so * sizeof(VT), static_cast<const VT*>(a.vals) + r0, kFastT * sizeof(VT), &full_bar[s], pol);
                 if (HAS_PRED) bulk_g2s(ring + sl.pred + so * PW, static_cast<const PL*>(a.pcol) + r0, kFastT * PW, &full_bar[s], pol);
@@ -729,8 +799,10 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
             fw.spill_out = a.spill_keys;
         }
         auto pass = [&](PL x) -> bool { return ((x >= plo) & (x <= phi)) != pinv; };
+        const uint8_t* kzb = reinterpret_cast<const uint8_t*>(sm + a.so_bar + 96);
         auto ring_row = [&](int g, uint64_t& kw, VT& v) {
             if constexpr (COMP) kw = composite_word(static_cast<int32_t>(rk0[g]), static_cast<int32_t>(rk1[g]));
+            else if constexpr (KZ) kw = key_word(kz_ring<KT>(ring + sl.key0, kzb, g, a.kz_off));
             else kw = key_word(rk0[g]);
             if constexpr (VALS) v = rv[g];
             else v = VT{};
@@ -797,7 +869,8 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                         act[u] = e < count;
                         const int i = HAS_PRED ? list[act[u] ? e : e0] : w0 + (act[u] ? e : e0);
                         if constexpr (COMP) kw[u] = composite_word(static_cast<int32_t>(k0p[i]), static_cast<int32_t>(k1p[i]));
-                        else kw[u] = key_word(a.kz ? kz_key<KT>(a, base + i) : k0p[i]);
+                        else if constexpr (KZ) kw[u] = key_word(kz_key<KT>(a, base + i));
+                        else kw[u] = key_word(k0p[i]);
                         if constexpr (VALS) v[u] = vp[i];
                         else v[u] = VT{};
                     }
@@ -807,18 +880,6 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                 continue;
             }
             if (!mbar_wait(&full_bar[s], ph, a.counters)) break;
-            if constexpr (!COMP) {
-                if (a.kz) {
-                    // Compressed keys: the warp unpacks its own rows' keys into the stage (no other warp reads them).
-                    KT* kd = reinterpret_cast<KT*>(ring + sl.key0) + s * kFastT;
-#pragma unroll
-                    for (int j = 0; j < kFastSeg; ++j) {
-                        const int r = warp * kFastR + 32 * j + lane;
-                        kd[r] = kz_key<KT>(a, tile * kFastT + r);
-                    }
-                    __syncwarp();
-                }
-            }
             const bool full = (q & 127) == 0 && __any_sync(0xffffffffu, table_full(a.counters));
             // The next tile of this CTA is staged too: rows left over may wait for it.
             const bool keep_going = carry && !full && q + 1 < my_tiles && tile + gridDim.x < a.full_tiles;
@@ -1089,19 +1150,29 @@ inline int fast_mode(const AggArgs& a) {
     return (mm | sum) ? (FM_VALS | mm | sum) : 0;
 }
 
+// The compressed-key variant exists for single keys other than DOUBLE; plain keys run the kernel without it.
+template <typename KT, bool COMP, typename VT, typename PT, int MODE>
+int32_t launch_fast_z(const AggArgs& a, size_t smem, cudaStream_t st) {
+    if constexpr (!COMP && !std::is_same<KT, double>::value) {
+        if (a.kz) return launch_fast_t<KT, COMP, VT, PT, MODE | FM_KZ>(a, smem, st);
+    }
+    if (a.kz) return fail(QDB_ERR_INVALID, "gb_fast_kernel: compressed keys need a single INT32, INT64 or FLOAT key");
+    return launch_fast_t<KT, COMP, VT, PT, MODE>(a, smem, st);
+}
+
 template <typename KT, bool COMP, typename VT, typename PT>
 int32_t launch_fast_m(const AggArgs& a, size_t smem, cudaStream_t st) {
     switch (fast_mode(a)) {
-        case FM_VALS | FM_SUM: return launch_fast_t<KT, COMP, VT, PT, FM_VALS | FM_SUM>(a, smem, st);
-        case FM_VALS | FM_MM: return launch_fast_t<KT, COMP, VT, PT, FM_VALS | FM_MM>(a, smem, st);
-        case FM_VALS | FM_SUM | FM_MM: return launch_fast_t<KT, COMP, VT, PT, FM_VALS | FM_SUM | FM_MM>(a, smem, st);
+        case FM_VALS | FM_SUM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM>(a, smem, st);
+        case FM_VALS | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_MM>(a, smem, st);
+        case FM_VALS | FM_SUM | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM | FM_MM>(a, smem, st);
         default: return fail(QDB_ERR_INVALID, "gb_fast_kernel: unsupported aggregate set");
     }
 }
 
 template <typename KT, bool COMP, typename PT>
 int32_t launch_fast_v(const AggArgs& a, ValKind vk, size_t smem, cudaStream_t st) {
-    if (fast_mode(a) == 0) return launch_fast_t<KT, COMP, int32_t, PT, 0>(a, smem, st);
+    if (fast_mode(a) == 0) return launch_fast_z<KT, COMP, int32_t, PT, 0>(a, smem, st);
     switch (vk) {
         case VK_I32: return launch_fast_m<KT, COMP, int32_t, PT>(a, smem, st);
         case VK_I64: return launch_fast_m<KT, COMP, int64_t, PT>(a, smem, st);
