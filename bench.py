@@ -71,6 +71,7 @@ def parse_args():
     ap.add_argument("--workload", default="filtered",
                     choices=["filtered", "batched", "served", "plain", "composite", "scalar", "string", "compressed"])
     ap.add_argument("--composite-rows", type=int, default=1 << 27)
+    ap.add_argument("--string-rows", type=int, default=1 << 25)
     ap.add_argument("--no-oracle", action="store_true",
                     help="plain / composite / scalar / string / compressed on their own: skip the oracle leg")
     ap.add_argument("--instances", type=int, default=BATCH_INSTANCES)
@@ -624,7 +625,7 @@ def string_and_order_measure(args, dev) -> tuple:
 
     from qikkdb_b200 import datagen as dg
     from qikkdb_b200.groupby import GPUString, StringGroupByTable, order_by
-    n, d = 1 << 25, 1 << 20
+    n, d = args.string_rows, 1 << 20
     chars, ends = string_columns(n, d, dev)
     vals_h = dg.uniform_i32(STR_SEED, 1, n, -1000, 1000)
     vals = torch.from_numpy(vals_h).to(dev)

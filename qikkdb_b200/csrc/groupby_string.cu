@@ -28,6 +28,7 @@
 // GetResults takes the numeric table's groups (slot number, NULL flag, aggregates) and rebuilds each key's string from
 // the records and the arena into a GPUString.
 #include "groupby_agg.cuh"
+#include "scan.cuh"
 
 namespace qdb {
 
@@ -79,15 +80,47 @@ __device__ __forceinline__ uint64_t gbs_key_word(const GbsDict& t, const GbsRec*
     return l2 ? __ldcg(a) : *a;
 }
 
+// Claims record r (slot pos) for the key (n bytes at byte offset b of W; w0..w2 its first three words, zero-padded)
+// and publishes it.  Kept out of line: the probe loop stays small, and claims are rare after a table fills.
+__device__ __noinline__ int64_t gbs_claim(GbsRec* r, uint64_t pos, uint64_t* arena, uint64_t arena_words,
+                                          unsigned long long* counters, const uint64_t* __restrict__ W, int64_t b,
+                                          int64_t n, uint64_t w0, uint64_t w1, uint64_t w2, unsigned* claims) {
+    atomicAdd(claims, 1u);
+    const int64_t words = (n + 7) >> 3;
+    const uint64_t extra = words > kGbsInline ? static_cast<uint64_t>(words - kGbsInline) : 0ull;
+    const unsigned long long o = extra ? atomicAdd(&counters[0], static_cast<unsigned long long>(extra)) : 0ull;
+    if (o + extra > arena_words) {
+        atomicExch(reinterpret_cast<int*>(&counters[1]), static_cast<int>(QDB_HASH_TABLE_FULL));
+        atomicExch(reinterpret_cast<unsigned long long*>(&r->meta), kMetaPoison);
+        return -1;
+    }
+    r->w[0] = w0;
+    r->w[1] = w1;
+    r->w[2] = w2;
+    for (int64_t j = kGbsInline; j < words; ++j) arena[o + (j - kGbsInline)] = gbs_word(W, b + 8 * j, n - 8 * j);
+    __threadfence();
+    atomicExch(reinterpret_cast<unsigned long long*>(&r->meta),
+               (static_cast<unsigned long long>(o) << 20) | static_cast<unsigned long long>(n + 1));
+    return static_cast<int64_t>(pos);
+}
+
 // Finds or claims the string at byte offset b (n bytes) of the buffer W; returns its slot, or -1 (table or arena
-// full, key too long, or a wait that gave up: the status word says which).
+// full, key too long, or a wait that gave up: the status word says which).  A key of at most 24 bytes lives in its
+// record: its three words (zero-padded) are hashed and compared without loops, the record read as two 16-byte loads.
 __device__ int64_t gbs_find(const GbsDict& t, const uint64_t* __restrict__ W, int64_t b, int64_t n, unsigned* claims) {
     if (n > kGbsMaxLen) {
         atomicExch(reinterpret_cast<int*>(&t.counters[1]), static_cast<int>(QDB_ERR_TOO_LARGE));
         return -1;
     }
+    const bool shortk = n <= 8 * kGbsInline;
+    uint64_t w[kGbsInline];
+#pragma unroll
+    for (int j = 0; j < kGbsInline; ++j) w[j] = 8 * j < n ? gbs_word(W, b + 8 * j, n - 8 * j) : 0ull;
     uint64_t h = 0x243F6A8885A308D3ull ^ (static_cast<uint64_t>(n) * 0xBF58476D1CE4E5B9ull);
-    for (int64_t j = 0; j < n; j += 8) h = gbs_round(h, gbs_word(W, b + j, n - j));
+#pragma unroll
+    for (int j = 0; j < kGbsInline; ++j)
+        if (8 * j < n) h = gbs_round(h, w[j]);
+    for (int64_t j = 8 * kGbsInline; j < n; j += 8) h = gbs_round(h, gbs_word(W, b + j, n - j));
     h = mix64(h);
     if (h == 0) h = 1;
     const int64_t words = (n + 7) >> 3;
@@ -98,47 +131,39 @@ __device__ int64_t gbs_find(const GbsDict& t, const uint64_t* __restrict__ W, in
         GbsRec* r = t.rec + pos;
         if (cur == 0) {
             cur = atomicCAS(reinterpret_cast<unsigned long long*>(t.header + pos), 0ull, h);
-            if (cur == 0) {  // claimed: store the key, then publish the meta word
-                atomicAdd(claims, 1u);
-                const uint64_t extra = words > kGbsInline ? static_cast<uint64_t>(words - kGbsInline) : 0ull;
-                const unsigned long long o =
-                    extra ? atomicAdd(&t.counters[0], static_cast<unsigned long long>(extra)) : 0ull;
-                if (o + extra > t.arena_words) {
-                    atomicExch(reinterpret_cast<int*>(&t.counters[1]), static_cast<int>(QDB_HASH_TABLE_FULL));
-                    atomicExch(reinterpret_cast<unsigned long long*>(&r->meta), kMetaPoison);
-                    return -1;
-                }
-                for (int64_t j = 0; j < words; ++j) {
-                    const uint64_t w = gbs_word(W, b + 8 * j, n - 8 * j);
-                    if (j < kGbsInline) r->w[j] = w;
-                    else t.arena[o + (j - kGbsInline)] = w;
-                }
-                __threadfence();
-                atomicExch(reinterpret_cast<unsigned long long*>(&r->meta),
-                           (static_cast<unsigned long long>(o) << 20) | static_cast<unsigned long long>(n + 1));
-                return static_cast<int64_t>(pos);
-            }
+            if (cur == 0) return gbs_claim(r, pos, t.arena, t.arena_words, t.counters, W, b, n, w[0], w[1], w[2], claims);
         }
         if (cur != h) continue;
         // Same hash: the published meta word, then the key.
-        uint64_t m = r->meta;
+        const ulonglong2* rq = reinterpret_cast<const ulonglong2*>(r);
+        ulonglong2 q0 = rq[0], q1 = rq[1];  // (meta, w0), (w1, w2)
         bool l2 = false;
-        for (uint32_t it = 0; m == 0 && it < kGbsWaitIters; ++it) {
+        for (uint32_t it = 0; q0.x == 0 && it < kGbsWaitIters; ++it) {
             __nanosleep(64);
-            m = ld_volatile_u64(&r->meta);
+            q0.x = ld_volatile_u64(&r->meta);
             l2 = true;  // the record's L1 copy predates the publication: read the key from L2
         }
+        const uint64_t m = q0.x;
         if (m == 0) {
             atomicExch(reinterpret_cast<int*>(&t.counters[1]), static_cast<int>(QDB_ERR_TIMEOUT));
             return -1;
         }
         if (m == kMetaPoison || gbs_meta_len(m) != n) continue;
-        bool eq = true;
-        for (int64_t j = 0; j < words && eq; ++j) eq = gbs_key_word(t, r, m, j, l2) == gbs_word(W, b + 8 * j, n - 8 * j);
+        if (l2) {
+            q0 = __ldcg(rq);
+            q1 = __ldcg(rq + 1);
+        }
+        bool eq = (q0.y == w[0]) & (q1.x == w[1]) & (q1.y == w[2]);
+        if (!shortk)
+            for (int64_t j = kGbsInline; j < words && eq; ++j)
+                eq = gbs_key_word(t, r, m, j, l2) == gbs_word(W, b + 8 * j, n - 8 * j);
         if (!eq && !l2) {
-            eq = true;
-            for (int64_t j = 0; j < words && eq; ++j)
-                eq = gbs_key_word(t, r, m, j, true) == gbs_word(W, b + 8 * j, n - 8 * j);
+            // a stale L1 copy cannot make a key miss its own slot: compare once more from L2
+            const ulonglong2 c0 = __ldcg(rq), c1 = __ldcg(rq + 1);
+            eq = (c0.y == w[0]) & (c1.x == w[1]) & (c1.y == w[2]);
+            if (!shortk)
+                for (int64_t j = kGbsInline; j < words && eq; ++j)
+                    eq = gbs_key_word(t, r, m, j, true) == gbs_word(W, b + 8 * j, n - 8 * j);
         }
         if (eq) return static_cast<int64_t>(pos);
     }
@@ -182,31 +207,6 @@ __global__ void gbs_len_kernel(GbsDict t, const int32_t* __restrict__ slots, con
         const bool isnull = knull && ((knull[r >> 6] >> (r & 63)) & 1ull);
         clen[r] = isnull ? 0 : static_cast<long long>(gbs_meta_len(t.rec[slots[r]].meta));
     }
-}
-
-// Exclusive scan of m int64 values in place by one block (chunks per thread, then the chunk sums).
-__global__ void __launch_bounds__(1024) gbs_scan_kernel(long long* v, int64_t m, long long* total) {
-    __shared__ long long part[1024];
-    const int64_t per = (m + 1023) / 1024;
-    const int64_t b = threadIdx.x * per;
-    const int64_t e = min(m, b + per);
-    long long sum = 0;
-    for (int64_t i = b; i < e; ++i) sum += v[i];
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (int d = 1; d < 1024; d <<= 1) {
-        const long long y = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
-        __syncthreads();
-        part[threadIdx.x] += y;
-        __syncthreads();
-    }
-    long long run = part[threadIdx.x] - sum;
-    for (int64_t i = b; i < e; ++i) {
-        const long long c = v[i];
-        v[i] = run;
-        run += c;
-    }
-    if (threadIdx.x == 1023) *total = part[1023];
 }
 
 // Result keys: group r's characters at cpos[r], its end offset cpos[r] + length.
@@ -397,11 +397,11 @@ int32_t qdb_gbs_results(qdb_gbs* g, int32_t n_aggs, const int32_t* aggs, char** 
     if (rc == QDB_OK) {
         const unsigned grid = gbs_grid(static_cast<uint64_t>(groups));
         gbs_len_kernel<<<grid, 256, 0, s>>>(g->t, static_cast<const int32_t*>(slots), knull, groups, clen);
-        gbs_scan_kernel<<<1, 1024, 0, s>>>(clen, groups, tot);
-        note_launch(2);
-        cudaError_t e = cudaMemcpyAsync(&nchars, tot, 8, cudaMemcpyDeviceToHost, s);
+        note_launch();
+        rc = exclusive_scan<long long>(clen, groups, tot, s);
+        cudaError_t e = rc == QDB_OK ? cudaMemcpyAsync(&nchars, tot, 8, cudaMemcpyDeviceToHost, s) : cudaSuccess;
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) rc = cuda_fail(e, "qdb_gbs_results: key lengths");
+        if (rc == QDB_OK && e != cudaSuccess) rc = cuda_fail(e, "qdb_gbs_results: key lengths");
     }
     if (rc == QDB_OK)
         rc = dev_alloc(reinterpret_cast<void**>(out_chars), static_cast<size_t>(std::max<long long>(nchars, 1)), s);

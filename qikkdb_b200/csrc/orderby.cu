@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "groupby.cuh"
+#include "scan.cuh"
 
 namespace qdb {
 
@@ -25,7 +26,6 @@ constexpr int kObThreads = 256;                      // 8 warps
 constexpr int kObItems = 8;                          // rows per thread in a tile
 constexpr int kObTile = kObThreads * kObItems;       // 2048 rows per tile
 constexpr int kObWarps = kObThreads / 32;
-constexpr int kObScanThreads = 1024;
 
 // Order-preserving unsigned encodings (ascending order of the value = ascending unsigned order).
 __device__ __forceinline__ uint32_t ob_enc(int32_t v) { return static_cast<uint32_t>(v) ^ 0x80000000u; }
@@ -78,31 +78,6 @@ __global__ void __launch_bounds__(kObThreads) ob_hist_kernel(const K* __restrict
     }
     __syncthreads();
     hist[static_cast<int64_t>(threadIdx.x) * tiles + blockIdx.x] = cnt[threadIdx.x];
-}
-
-// Exclusive scan of m counts in place, by one block: each thread sums a contiguous chunk, the block scans the
-// chunk sums, then each thread rewrites its chunk.
-__global__ void __launch_bounds__(kObScanThreads) ob_scan_kernel(int32_t* __restrict__ v, int64_t m) {
-    __shared__ int32_t part[kObScanThreads];
-    const int64_t per = (m + kObScanThreads - 1) / kObScanThreads;
-    const int64_t b = threadIdx.x * per;
-    const int64_t e = min(m, b + per);
-    int32_t s = 0;
-    for (int64_t i = b; i < e; ++i) s += v[i];
-    part[threadIdx.x] = s;
-    __syncthreads();
-    for (int d = 1; d < kObScanThreads; d <<= 1) {  // inclusive Hillis-Steele scan of the chunk sums
-        const int32_t y = threadIdx.x >= d ? part[threadIdx.x - d] : 0;
-        __syncthreads();
-        part[threadIdx.x] += y;
-        __syncthreads();
-    }
-    int32_t run = part[threadIdx.x] - s;
-    for (int64_t i = b; i < e; ++i) {
-        const int32_t c = v[i];
-        v[i] = run;
-        run += c;
-    }
 }
 
 // Stable scatter of one tile: row i of the tile (in row order: warp w holds rows [256 w, 256 w + 256), step j of
@@ -196,8 +171,8 @@ static int32_t ob_radix(K* ka, int32_t* ia, K* kb, int32_t* ib, int64_t n, int32
     for (int shift = 0; shift < static_cast<int>(8 * sizeof(K)); shift += 8) {
         ob_hist_kernel<K><<<static_cast<unsigned>(tiles), kObThreads, 0, s>>>(ka, n, shift, hist, tiles);
         note_launch();
-        ob_scan_kernel<<<1, kObScanThreads, 0, s>>>(hist, 256 * tiles);
-        note_launch();
+        const int32_t rc = exclusive_scan<int32_t>(hist, 256 * tiles, nullptr, s);
+        if (rc != QDB_OK) return rc;
         ob_scatter_kernel<K><<<static_cast<unsigned>(tiles), kObThreads, 0, s>>>(ka, ia, n, shift, hist, tiles, kb, ib);
         note_launch();
         std::swap(ka, kb);
