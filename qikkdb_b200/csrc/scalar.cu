@@ -12,6 +12,7 @@
 // the calls of a query's blocks.  Results follow the GROUP BY operator's types: V for MIN/MAX/SUM/AVG (an integer SUM
 // wraps in V, an integer AVG truncates), int64 for COUNT; MIN/MAX/SUM/AVG over no row are NULL.
 #include <climits>
+#include <limits>
 
 #include "groupby_agg.cuh"
 
@@ -26,14 +27,34 @@ struct ScalarState {            // device accumulator of one scalar query
 
 constexpr int kScThreads = 256;
 
+// Order-preserving encoding of a value in the narrowest integer that holds it (32 bits for 4-byte types).
 template <typename VT>
-__device__ __forceinline__ long long sc_enc(VT v) {
+using EncT = typename std::conditional<sizeof(VT) == 4, int32_t, long long>::type;
+
+template <typename VT>
+__device__ __forceinline__ EncT<VT> sc_enc(VT v) {
     if constexpr (std::is_same<VT, float>::value) return fenc(v);
     else if constexpr (std::is_same<VT, double>::value) return denc(v);
-    else return static_cast<long long>(v);
+    else return static_cast<EncT<VT>>(v);
 }
 
-template <typename VT, typename PT>
+// Four consecutive elements from a 16-byte aligned address (streaming loads: read once).
+template <typename T>
+__device__ __forceinline__ void load4(const T* p, T (&o)[4]) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    if constexpr (sizeof(T) == 4) {
+        const uint4 a = __ldcs(q);
+        memcpy(o, &a, 16);
+    } else {
+        const uint4 a = __ldcs(q), b = __ldcs(q + 1);
+        memcpy(o, &a, 16);
+        memcpy(o + 2, &b, 16);
+    }
+}
+
+// VEC: the value and predicate columns start on 16-byte boundaries, so each thread takes four consecutive rows per
+// step with vector loads (two steps in flight); otherwise four rows strided by the grid per step.
+template <typename VT, typename PT, bool VEC>
 __global__ void __launch_bounds__(kScThreads) scalar_kernel(const VT* __restrict__ vals, const uint64_t* __restrict__ vnull,
                                                             int64_t n, const PT* __restrict__ pcol,
                                                             const uint64_t* __restrict__ pnull, PredInterval pi,
@@ -41,11 +62,23 @@ __global__ void __launch_bounds__(kScThreads) scalar_kernel(const VT* __restrict
     constexpr bool HAS_PRED = !std::is_same<PT, NoPred>::value;
     constexpr bool VFLOAT = std::is_floating_point<VT>::value;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
+    using ET = EncT<VT>;
+    // An int32 sum is kept mod 2^32 per thread: the result wraps in the value type.
+    using ST = typename std::conditional<sizeof(VT) == 4, unsigned int, unsigned long long>::type;
     const PL plo = HAS_PRED ? from_bits<PL>(pi.lo) : PL{};
     const PL phi = HAS_PRED ? from_bits<PL>(pi.hi) : PL{};
-    unsigned long long cnt = 0, isum = 0;
+    unsigned int cnt = 0;
+    ST isum = 0;
     double fsum = 0.0;
-    long long mn = LLONG_MAX, mx = LLONG_MIN;
+    ET mn = std::numeric_limits<ET>::max(), mx = std::numeric_limits<ET>::min();
+    auto take = [&](VT v) {
+        ++cnt;
+        if constexpr (VFLOAT) fsum += static_cast<double>(v);
+        else isum += static_cast<ST>(v);
+        const ET e = sc_enc(v);
+        mn = min(mn, e);
+        mx = max(mx, e);
+    };
     auto row = [&](int64_t i, PL x, VT v) {
         bool keep = true;
         if constexpr (HAS_PRED) {
@@ -54,65 +87,108 @@ __global__ void __launch_bounds__(kScThreads) scalar_kernel(const VT* __restrict
         }
         if (mask) keep = keep && mask[i] != 0;
         if (vnull) keep = keep && !((vnull[i >> 6] >> (i & 63)) & 1ull);
-        if (!keep) return;
-        ++cnt;
-        if constexpr (VFLOAT) fsum += static_cast<double>(v);
-        else isum += static_cast<unsigned long long>(static_cast<long long>(v));
-        const long long e = sc_enc(v);
-        mn = min(mn, e);
-        mx = max(mx, e);
+        if (keep) take(v);
     };
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-    // Four rows per thread and step, all loads issued before any is used, so that enough bytes are in flight per SM
-    // to cover the memory latency at full bandwidth.
-    constexpr int U = 4;
-    for (; i + (U - 1) * stride < n; i += U * stride) {
-        PL x[U];
-        VT v[U];
+    const int64_t tid = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if constexpr (VEC) {
+        const int64_t chunks = n >> 2;
+        auto chunk = [&](int64_t c, const VT (&v)[4], const PL (&x)[4]) {
+            const int64_t i = c << 2;
+            // the four rows' NULL and mask flags as bits 0..3
+            unsigned drop = 0;
+            if (pnull) drop |= static_cast<unsigned>(pnull[i >> 6] >> (i & 63)) & 15u;
+            if (vnull) drop |= static_cast<unsigned>(vnull[i >> 6] >> (i & 63)) & 15u;
+            if (mask)
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            x[u] = HAS_PRED ? __ldcs(reinterpret_cast<const PL*>(pcol) + i + u * stride) : PL{};
-            v[u] = __ldcs(vals + i + u * stride);
+                for (int u = 0; u < 4; ++u) drop |= (mask[i + u] == 0 ? 1u : 0u) << u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                bool keep = !((drop >> u) & 1u);
+                if constexpr (HAS_PRED) keep = keep && (((x[u] >= plo) & (x[u] <= phi)) != (pi.invert != 0));
+                if (keep) take(v[u]);
+            }
+        };
+        int64_t c = tid;
+        for (; c + stride < chunks; c += 2 * stride) {
+            VT v0[4], v1[4];
+            PL x0[4], x1[4];
+            load4(vals + (c << 2), v0);
+            load4(vals + ((c + stride) << 2), v1);
+            if constexpr (HAS_PRED) {
+                load4(reinterpret_cast<const PL*>(pcol) + (c << 2), x0);
+                load4(reinterpret_cast<const PL*>(pcol) + ((c + stride) << 2), x1);
+            }
+            chunk(c, v0, x0);
+            chunk(c + stride, v1, x1);
         }
+        for (; c < chunks; c += stride) {
+            VT v0[4];
+            PL x0[4];
+            load4(vals + (c << 2), v0);
+            if constexpr (HAS_PRED) load4(reinterpret_cast<const PL*>(pcol) + (c << 2), x0);
+            chunk(c, v0, x0);
+        }
+        for (int64_t i = (chunks << 2) + tid; i < n; i += stride)
+            row(i, HAS_PRED ? reinterpret_cast<const PL*>(pcol)[i] : PL{}, vals[i]);
+    } else {
+        int64_t i = tid;
+        // Four rows per thread and step, all loads issued before any is used, so that enough bytes are in flight per
+        // SM to cover the memory latency at full bandwidth.
+        constexpr int U = 4;
+        for (; i + (U - 1) * stride < n; i += U * stride) {
+            PL x[U];
+            VT v[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) row(i + u * stride, x[u], v[u]);
+            for (int u = 0; u < U; ++u) {
+                x[u] = HAS_PRED ? __ldcs(reinterpret_cast<const PL*>(pcol) + i + u * stride) : PL{};
+                v[u] = __ldcs(vals + i + u * stride);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) row(i + u * stride, x[u], v[u]);
+        }
+        for (; i < n; i += stride) row(i, HAS_PRED ? reinterpret_cast<const PL*>(pcol)[i] : PL{}, vals[i]);
     }
-    for (; i < n; i += stride) row(i, HAS_PRED ? reinterpret_cast<const PL*>(pcol)[i] : PL{}, vals[i]);
     // warp, then block reduce
+    unsigned long long c64 = cnt, s64 = isum;
+    long long mn64 = mn, mx64 = mx;
+    if (cnt == 0) {
+        mn64 = LLONG_MAX;
+        mx64 = LLONG_MIN;
+    }
     for (int d = 16; d > 0; d >>= 1) {
-        cnt += __shfl_down_sync(0xffffffffu, cnt, d);
-        isum += __shfl_down_sync(0xffffffffu, isum, d);
+        c64 += __shfl_down_sync(0xffffffffu, c64, d);
+        s64 += __shfl_down_sync(0xffffffffu, s64, d);
         fsum += __shfl_down_sync(0xffffffffu, fsum, d);
-        mn = min(mn, __shfl_down_sync(0xffffffffu, mn, d));
-        mx = max(mx, __shfl_down_sync(0xffffffffu, mx, d));
+        mn64 = min(mn64, __shfl_down_sync(0xffffffffu, mn64, d));
+        mx64 = max(mx64, __shfl_down_sync(0xffffffffu, mx64, d));
     }
     __shared__ unsigned long long s_cnt[kScThreads / 32], s_isum[kScThreads / 32];
     __shared__ double s_fsum[kScThreads / 32];
     __shared__ long long s_mn[kScThreads / 32], s_mx[kScThreads / 32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
-        s_cnt[warp] = cnt;
-        s_isum[warp] = isum;
+        s_cnt[warp] = c64;
+        s_isum[warp] = s64;
         s_fsum[warp] = fsum;
-        s_mn[warp] = mn;
-        s_mx[warp] = mx;
+        s_mn[warp] = mn64;
+        s_mx[warp] = mx64;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < kScThreads / 32; ++w) {
-            cnt += s_cnt[w];
-            isum += s_isum[w];
+            c64 += s_cnt[w];
+            s64 += s_isum[w];
             fsum += s_fsum[w];
-            mn = min(mn, s_mn[w]);
-            mx = max(mx, s_mx[w]);
+            mn64 = min(mn64, s_mn[w]);
+            mx64 = max(mx64, s_mx[w]);
         }
-        if (cnt) {
-            atomicAdd(&st->count, cnt);
+        if (c64) {
+            atomicAdd(&st->count, c64);
             if (VFLOAT) atomicAdd(&st->fsum, fsum);
-            else atomicAdd(&st->isum, isum);
-            atomicMin(&st->mn, mn);
-            atomicMax(&st->mx, mx);
+            else atomicAdd(&st->isum, s64);
+            atomicMin(&st->mn, mn64);
+            atomicMax(&st->mx, mx64);
         }
     }
 }
@@ -121,18 +197,19 @@ template <typename VT, typename PT>
 static void scalar_launch(const void* vals, const uint64_t* vnull, int64_t n, const void* pcol, const uint64_t* pnull,
                           const PredInterval& pi, const int8_t* mask, ScalarState* st, cudaStream_t s) {
     const DeviceInfo& di = device_info();
+    const bool vec = (reinterpret_cast<uintptr_t>(vals) & 15u) == 0 && (reinterpret_cast<uintptr_t>(pcol) & 15u) == 0;
+    auto kern = vec ? scalar_kernel<VT, PT, true> : scalar_kernel<VT, PT, false>;
     // One wave: as many blocks as are resident on every SM at once.
-    static int per_sm = 0;
-    if (per_sm == 0) {
+    static int per_sm[2] = {0, 0};
+    if (per_sm[vec] == 0) {
         int b = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, scalar_kernel<VT, PT>, kScThreads, 0) != cudaSuccess || b < 1)
-            b = 4;
-        per_sm = b;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kScThreads, 0) != cudaSuccess || b < 1) b = 4;
+        per_sm[vec] = b;
     }
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(
-        1, std::min<int64_t>((n + kScThreads - 1) / kScThreads, int64_t(di.sm_count) * per_sm)));
-    scalar_kernel<VT, PT><<<grid, kScThreads, 0, s>>>(static_cast<const VT*>(vals), vnull, n,
-                                                       static_cast<const PT*>(pcol), pnull, pi, mask, st);
+        1, std::min<int64_t>((n + kScThreads - 1) / kScThreads, int64_t(di.sm_count) * per_sm[vec])));
+    kern<<<grid, kScThreads, 0, s>>>(static_cast<const VT*>(vals), vnull, n, static_cast<const PT*>(pcol), pnull, pi,
+                                     mask, st);
     note_launch();
 }
 
