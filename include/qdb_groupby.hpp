@@ -12,6 +12,8 @@
  *                    CompressNullMask}   GPUReconstruct.cuh:204-640
  *   GPUOrderBy::{OrderByColumn, ReOrderByIdx, ReOrderNullValuesByIdx}   GPUOrderBy.cuh:88-195
  *   GPUAggregation::col<AGG, OUT, IN>      GPUAggregation.cuh:15-37
+ *   CompressionGPU::{compressDataAAFL, decompressDataAAFL, decompressDataAAFLOnDevice}
+ *                                          qikkDB/Compression/GPUCompression.h:10-80
  *   GPUMemory::{alloc, allocAndSet, free, copyHostToDevice, copyDeviceToHost, copyDeviceToDevice, memset}
  *                                          GPUMemory.cuh:18-236
  *   query_engine_error / gpu_error / QueryEngineErrorType   qikkDB/QueryEngine/GPUError.h:17-75
@@ -28,6 +30,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -783,6 +786,84 @@ private:
     int32_t n_;
     int32_t* indices_ = nullptr;
     bool first_ = true;
+};
+
+/* ---- CompressionGPU (qikkDB/Compression/GPUCompression.h:10-80): AAFL column blocks ----
+ * The same block format (header, position ids, bit lengths, packed words); compression and decompression run on the
+ * GPU.  Supported element types: int32_t, int64_t and float (single-sign blocks); other types return false, as the
+ * reference does for double.  A block that would not shrink is not compressed (false). */
+class CompressionGPU {
+    template <typename T>
+    static int32_t code() {
+        return std::is_same<T, int32_t>::value ? QDB_INT32
+               : std::is_same<T, int64_t>::value ? QDB_INT64
+               : std::is_same<T, float>::value   ? QDB_FLOAT
+                                                 : 0;
+    }
+    template <typename T>
+    static int64_t bits(T v) {
+        if (sizeof(T) == 8) {
+            int64_t b;
+            std::memcpy(&b, &v, 8);
+            return b;
+        }
+        int32_t b;
+        std::memcpy(&b, &v, 4);
+        return b;
+    }
+
+public:
+    static const char CWARP_SIZE = 32;
+
+    /* compressDataAAFL (GPUCompression.cu:150-225): host column in, host block out. */
+    template <typename T>
+    static bool compressDataAAFL(T* const hostUncompressed, int64_t uncompressedElementsCount,
+                                 std::vector<T>& hostCompressed, int64_t& compressedElementsCount, T minValue,
+                                 T maxValue) {
+        if (code<T>() == 0 || uncompressedElementsCount <= 0) return false;
+        cuda_ptr<T> d(static_cast<size_t>(uncompressedElementsCount));
+        GPUMemory::copyHostToDevice(d.get(), hostUncompressed, static_cast<size_t>(uncompressedElementsCount));
+        void* blk = nullptr;
+        int64_t elems = 0;
+        qdb_cpp::check(qdb_aafl_compress(code<T>(), d.get(), uncompressedElementsCount, bits(minValue), bits(maxValue),
+                                         &blk, &elems, nullptr));
+        if (!blk) return false;
+        hostCompressed.resize(static_cast<size_t>(elems));
+        GPUMemory::copyDeviceToHost(hostCompressed.data(), static_cast<const T*>(blk), static_cast<size_t>(elems));
+        GPUMemory::free(blk);
+        compressedElementsCount = elems;
+        return true;
+    }
+
+    /* decompressDataAAFLOnDevice (GPUCompression.cu:474-522): a device block into a device column. */
+    template <typename T>
+    static bool decompressDataAAFLOnDevice(T* const deviceCompressed, int64_t uncompressedElementsCount,
+                                           int64_t compressedElementsCount, int64_t compressionBlocksCount,
+                                           T* const deviceUncompressed, T minValue, T maxValue) {
+        if (code<T>() == 0) return false;
+        qdb_aafl_col c{deviceCompressed, code<T>(), 0, uncompressedElementsCount, compressedElementsCount,
+                       compressionBlocksCount, bits(minValue), bits(maxValue)};
+        qdb_cpp::check(qdb_aafl_decompress(&c, deviceUncompressed, nullptr));
+        return true;
+    }
+
+    /* decompressDataAAFL (GPUCompression.cu:366-440): host block in (its header gives the counts), host column out. */
+    template <typename T>
+    static bool decompressDataAAFL(T* const hostCompressed, int64_t compressedElementsCount,
+                                   std::vector<T>& hostUncompressed, int64_t& uncompressedElementsCount, T minValue,
+                                   T maxValue) {
+        if (code<T>() == 0 || compressedElementsCount * static_cast<int64_t>(sizeof(T)) < 24) return false;
+        int64_t hdr[3];
+        std::memcpy(hdr, hostCompressed, 24);
+        cuda_ptr<T> blk(static_cast<size_t>(compressedElementsCount));
+        GPUMemory::copyHostToDevice(blk.get(), hostCompressed, static_cast<size_t>(compressedElementsCount));
+        cuda_ptr<T> out(static_cast<size_t>(hdr[0] > 0 ? hdr[0] : 1));
+        decompressDataAAFLOnDevice(blk.get(), hdr[0], hdr[1], hdr[2], out.get(), minValue, maxValue);
+        hostUncompressed.resize(static_cast<size_t>(hdr[0]));
+        GPUMemory::copyDeviceToHost(hostUncompressed.data(), out.get(), static_cast<size_t>(hdr[0]));
+        uncompressedElementsCount = hdr[0];
+        return true;
+    }
 };
 
 #endif /* QDB_GROUPBY_HPP */

@@ -12,11 +12,13 @@
 //   then the key columns, the key null flags (when given), the values, the value null flags and the predicate
 //   column (when given), <rows> numbers each.
 // Output, per case:  "result <name> <groups> <multiplier>", then per group "<key...> <key null...> <value null> <value>".
-// With the single argument "version" it prints the library version and exits (no GPU needed); "order", "scalar" and
-// "string" run the ORDER BY, scalar-aggregation and string-key GROUP BY operators (described at their functions).
+// With the single argument "version" it prints the library version and exits (no GPU needed); "order", "scalar",
+// "string" and "compress" run the ORDER BY, scalar-aggregation, string-key GROUP BY and compressed-block operators
+// (described at their functions).
 #include <cstdint>
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <iostream>
 #include <string>
 #include <vector>
@@ -407,6 +409,48 @@ int run_string() {
     return 0;
 }
 
+// "compress" mode: CompressionGPU on the columns of GPUCompressionTests.cpp.  Input per case: "<type code> <rows>" and
+// the values.  Output: "plain", or "block" and the block's first eight words (int32 words for 4-byte types, int64
+// for 8-byte ones), then "roundtrip <1|0>" from decompressDataAAFL (host) and decompressDataAAFLOnDevice.
+template <typename T, typename Word>
+void compress_case(int32_t n) {
+    std::vector<T> v(n);
+    for (auto& x : v) std::cin >> x;
+    const T mn = *std::min_element(v.begin(), v.end()), mx = *std::max_element(v.begin(), v.end());
+    std::vector<T> blk;
+    int64_t elems = 0;
+    if (!CompressionGPU::compressDataAAFL(v.data(), n, blk, elems, mn, mx)) {
+        std::printf("plain\n");
+        return;
+    }
+    std::printf("block");
+    const Word* w = reinterpret_cast<const Word*>(blk.data());
+    for (int i = 0; i < 8; ++i) std::printf(" %lld", static_cast<long long>(w[i]));
+    std::printf("\n");
+    std::vector<T> back;
+    int64_t rows = 0;
+    bool ok = CompressionGPU::decompressDataAAFL(blk.data(), elems, back, rows, mn, mx) && rows == n &&
+              std::memcmp(back.data(), v.data(), sizeof(T) * static_cast<size_t>(n)) == 0;
+    int64_t hdr[3];
+    std::memcpy(hdr, blk.data(), 24);
+    cuda_ptr<T> db(static_cast<size_t>(elems)), out(static_cast<size_t>(n));
+    GPUMemory::copyHostToDevice(db.get(), blk.data(), static_cast<size_t>(elems));
+    ok = ok && CompressionGPU::decompressDataAAFLOnDevice(db.get(), hdr[0], hdr[1], hdr[2], out.get(), mn, mx);
+    std::vector<T> dev = to_host(out.get(), n);
+    ok = ok && std::memcmp(dev.data(), v.data(), sizeof(T) * static_cast<size_t>(n)) == 0;
+    std::printf("roundtrip %d\n", ok ? 1 : 0);
+}
+
+int run_compress() {
+    int32_t type = 0, n = 0;
+    while (std::cin >> type >> n) {
+        if (type == COLUMN_INT) compress_case<int32_t, int32_t>(n);
+        else if (type == COLUMN_LONG) compress_case<int64_t, int64_t>(n);
+        else compress_case<float, int32_t>(n);
+    }
+    return 0;
+}
+
 int main(int argc, char** argv) {
     if (argc > 1 && std::string(argv[1]) == "version") {
         std::printf("%s\n", qdb_version());
@@ -416,6 +460,7 @@ int main(int argc, char** argv) {
         if (argc > 1 && std::string(argv[1]) == "order") return run_order();
         if (argc > 1 && std::string(argv[1]) == "scalar") return run_scalar();
         if (argc > 1 && std::string(argv[1]) == "string") return run_string();
+        if (argc > 1 && std::string(argv[1]) == "compress") return run_compress();
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 2;

@@ -180,3 +180,33 @@ def test_dropin_string_groupby(cuda):
             got[key] = None if v == "N" else int(v)
         assert got == string_expected(c), (name, got)
         i += 1 + int(g)
+
+
+@pytest.mark.gpu
+def test_dropin_compression_reference_columns(cuda):
+    """CompressionGPU::compressDataAAFL / decompressDataAAFL / decompressDataAAFLOnDevice through the C++ drop-in on the
+    columns of qikkDB_test/GPUCompressionTests.cpp: the header words the tests assert, the blocks left plain, and
+    the round trip."""
+    from kat_util import compression_column, load_compression_kats
+    exe = build_program()
+    cases = load_compression_kats()
+    codes = {np.dtype(np.int32): 8, np.dtype(np.int64): 9, np.dtype(np.float32): 10}
+    text = ""
+    for c in cases:
+        v = compression_column(c["name"])
+        vals = " ".join(repr(float(x)) if v.dtype.kind == "f" else str(int(x)) for x in v)
+        text += f"{codes[v.dtype]} {len(v)}\n{vals}\n"
+    r = subprocess.run([exe, "compress"], input=text, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    i = 0
+    for c in cases:
+        want = c.get("head32", c.get("head64"))
+        if want == "plain":
+            assert lines[i] == "plain", c["name"]
+            i += 1
+            continue
+        parts = lines[i].split()
+        assert parts[0] == "block" and [int(x) for x in parts[1:]] == want, (c["name"], lines[i])
+        assert lines[i + 1] == "roundtrip 1", c["name"]
+        i += 2
