@@ -343,6 +343,18 @@ int32_t qdb_gbs_reset(qdb_gbs* g, void* stream);
 int32_t qdb_gbs_process(qdb_gbs* g, const char* chars, const int64_t* ends, const uint64_t* key_nulls, const void* vals,
                         const uint64_t* val_nulls, const int8_t* mask, int64_t n, void* stream);
 int32_t qdb_gbs_check(qdb_gbs* g, void* stream);
+/* The partial state of a string table, for GetResults over several GPUs' tables (GPUGroupByString.cuh:565-785, which
+ * gathers every table's keys and values on the host): qdb_gbs_export writes every group as a record (its key string
+ * into a newly allocated GPUString *out_chars / *out_ends, the NULL key as an empty string, and the numeric table's
+ * state words and flags as qdb_gb_export_partitioned lays them out) and synchronises `stream`;
+ * qdb_gbs_merge_exported adds `n` such records, copied to this table's device, into `g` (asynchronous; overflow
+ * latches QDB_HASH_TABLE_FULL for qdb_gbs_check). */
+int32_t qdb_gbs_export(qdb_gbs* g, char** out_chars, int64_t** out_ends, uint64_t** out_state, uint8_t** out_flags,
+                       int64_t* out_count, void* stream);
+int32_t qdb_gbs_merge_exported(qdb_gbs* g, const char* chars, const int64_t* ends, const uint64_t* state,
+                               const uint8_t* flags, int64_t n, void* stream);
+/* State words per exported record of `g` (the size of *out_state is count times this). */
+int32_t qdb_gbs_state_words(qdb_gbs* g, int32_t* out_words);
 int32_t qdb_gbs_results(qdb_gbs* g, int32_t n_aggs, const int32_t* aggs, char** out_chars, int64_t** out_ends,
                         uint64_t** out_key_nulls, void** out_vals, uint64_t** out_val_nulls, int64_t* out_count,
                         void* stream);

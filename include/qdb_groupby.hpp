@@ -551,7 +551,7 @@ public:
     /* GPUGroupBy(maxHashCount, keySizeMultiplier) (GPUGroupByString.cuh:210): up to
      * min(maxHashCount * keySizeMultiplier, 2^30) distinct non-NULL keys, plus the NULL key. */
     GPUGroupBy(const int32_t maxHashCount, const int32_t keySizeMultiplier)
-        : max_groups_(qdb_cpp::table_size(maxHashCount, keySizeMultiplier)) {
+        : max_groups_(qdb_cpp::table_size(maxHashCount, keySizeMultiplier)), device_(qdb_cpp::current_device()) {
         qdb_cpp::check(qdb_gbs_create(&g_, AGG::bit, AGG::bit ? qdb_cpp::type_of<V>::code : 0, max_groups_, 0, nullptr));
     }
     ~GPUGroupBy() {
@@ -591,9 +591,75 @@ public:
         if (outValuesNullMask) *outValuesNullMask = reinterpret_cast<nullmask_t*>(vn);
     }
 
+    /* GetResults over the tables of every GPU (GPUGroupByString.cuh:565): every table's groups (key strings and
+     * partial states) are merged into a new table on the current GPU, whose results are returned. */
+    void GetResults(GPUMemory::GPUString* outKeys, O** outValues, int32_t* outDataElementCount,
+                    std::vector<std::unique_ptr<IGroupBy>>& tables, nullmask_t** outKeysNullMask = nullptr,
+                    nullmask_t** outValuesNullMask = nullptr) {
+        if (tables.size() <= 1) {
+            GetResults(outKeys, outValues, outDataElementCount, outKeysNullMask, outValuesNullMask);
+            return;
+        }
+        int64_t groups = 0;
+        for (auto& tb : tables) groups += static_cast<GPUGroupBy*>(tb.get())->max_groups_;
+        GPUGroupBy merged(static_cast<int32_t>(groups < INT32_MAX ? groups : INT32_MAX), 1);
+        for (auto& tb : tables) merged.merge_from(*static_cast<GPUGroupBy*>(tb.get()));
+        merged.GetResults(outKeys, outValues, outDataElementCount, outKeysNullMask, outValuesNullMask);
+    }
+
 private:
+    /* Adds every group of `src` (on any GPU) to this table. */
+    void merge_from(GPUGroupBy& src) {
+        char* chars = nullptr;
+        int64_t* ends = nullptr;
+        uint64_t* state = nullptr;
+        uint8_t* flags = nullptr;
+        int64_t n = 0;
+        int32_t words = 0;
+        {
+            qdb_cpp::device_guard g(src.device_);
+            qdb_cpp::check(qdb_gbs_export(src.g_, &chars, &ends, &state, &flags, &n, nullptr));
+            qdb_cpp::check(qdb_gbs_state_words(src.g_, &words));
+        }
+        if (n == 0) return;
+        if (src.device_ == device_) {
+            qdb_cpp::check(qdb_gbs_merge_exported(g_, chars, ends, state, flags, n, nullptr));
+            qdb_cpp::check(qdb_gbs_check(g_, nullptr));
+            GPUMemory::free(chars);
+            GPUMemory::free(ends);
+            GPUMemory::free(state);
+            GPUMemory::free(flags);
+            return;
+        }
+        /* records of another GPU are copied into this GPU's memory first, then released on their own GPU */
+        int64_t nchars = 0;
+        {
+            qdb_cpp::device_guard g(src.device_);
+            GPUMemory::copyDeviceToHost(&nchars, ends + (n - 1), 1);
+        }
+        cuda_ptr<char> c(static_cast<size_t>(nchars > 0 ? nchars : 1));
+        cuda_ptr<int64_t> e(static_cast<size_t>(n));
+        cuda_ptr<uint64_t> st(static_cast<size_t>(n) * static_cast<size_t>(words > 0 ? words : 1));
+        cuda_ptr<uint8_t> f(static_cast<size_t>(n));
+        if (nchars > 0) qdb_cpp::check(qdb_memcpy_peer(c.get(), device_, chars, src.device_, nchars));
+        qdb_cpp::check(qdb_memcpy_peer(e.get(), device_, ends, src.device_, n * 8));
+        if (words > 0) qdb_cpp::check(qdb_memcpy_peer(st.get(), device_, state, src.device_, n * words * 8));
+        qdb_cpp::check(qdb_memcpy_peer(f.get(), device_, flags, src.device_, n));
+        {
+            qdb_cpp::device_guard g(src.device_);
+            GPUMemory::free(chars);
+            GPUMemory::free(ends);
+            GPUMemory::free(state);
+            GPUMemory::free(flags);
+            qdb_cpp::sync();
+        }
+        qdb_cpp::check(qdb_gbs_merge_exported(g_, c.get(), e.get(), st.get(), f.get(), n, nullptr));
+        qdb_cpp::check(qdb_gbs_check(g_, nullptr));
+    }
+
     qdb_gbs* g_ = nullptr;
     int64_t max_groups_;
+    int32_t device_;
 };
 
 /* Releases the key columns returned by the multi-key GetResults (GPUGroupByMultiKey.cu:403-418). */

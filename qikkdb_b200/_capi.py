@@ -185,6 +185,9 @@ SIGNATURES = [
     ("qdb_gbs_process", I32, [P, P, P, P, P, P, P, I64, P]),
     ("qdb_gbs_check", I32, [P, P]),
     ("qdb_gbs_results", I32, [P, I32, P, PP, PP, PP, PP, PP, C.POINTER(I64), P]),
+    ("qdb_gbs_export", I32, [P, PP, PP, PP, PP, C.POINTER(I64), P]),
+    ("qdb_gbs_merge_exported", I32, [P, P, P, P, P, I64, P]),
+    ("qdb_gbs_state_words", I32, [P, C.POINTER(I32)]),
     ("qdb_aafl_decompress", I32, [C.POINTER(qdb_aafl_col), P, P]),
     ("qdb_aafl_compress", I32, [I32, P, I64, I64, I64, PP, C.POINTER(I64), P]),
     ("qdb_gb_process_aafl", I32, [P, C.POINTER(qdb_aafl_col), P, C.POINTER(qdb_pred), P]),

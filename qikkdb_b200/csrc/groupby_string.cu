@@ -232,6 +232,35 @@ __global__ void gbs_emit_kernel(GbsDict t, const int32_t* __restrict__ slots, co
     }
 }
 
+// The keys of `groups` slots (knull bit set: the NULL key, an empty string) as a newly allocated GPUString.
+static int32_t gbs_build_keys(const GbsDict& t, const int32_t* slots, const uint64_t* knull, int64_t groups,
+                              char** out_chars, int64_t** out_ends, cudaStream_t s);
+
+// Export records: slot numbers from the numeric table's key words, and the NULL-key flag as a bitmask.
+__global__ void gbs_export_prep_kernel(const uint64_t* __restrict__ keys, const uint8_t* __restrict__ flags, int64_t n,
+                                       int32_t* __restrict__ slots, unsigned long long* __restrict__ knull) {
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const bool isnull = (flags[r] & 1u) != 0;  // bit 0 of the export flags: the NULL-key slot
+        slots[r] = isnull ? 0 : static_cast<int32_t>(keys[r]);
+        if (isnull) atomicOr(knull + (r >> 6), 1ull << (r & 63));
+    }
+}
+
+// Merge of exported records: rows whose record is the NULL key are left out of the dictionary pass (mask 0); the
+// slot numbers the pass returns become the numeric table's key words.
+__global__ void gbs_merge_prep_kernel(const uint8_t* __restrict__ flags, int64_t n, int8_t* __restrict__ mask) {
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        mask[r] = (flags[r] & 1u) ? 0 : 1;
+}
+
+__global__ void gbs_keywords_kernel(const int32_t* __restrict__ ids, int64_t n, uint64_t* __restrict__ keys) {
+    for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+         r += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        keys[r] = static_cast<uint64_t>(static_cast<int64_t>(ids[r]));  // the int32 key word
+}
+
 static uint64_t gbs_pow2(uint64_t x) {
     uint64_t p = 16;
     while (p < x) p <<= 1;
@@ -241,6 +270,43 @@ static uint64_t gbs_pow2(uint64_t x) {
 static unsigned gbs_grid(uint64_t n) {
     const DeviceInfo& di = device_info();
     return static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, uint64_t(di.sm_count) * 8)));
+}
+
+static int32_t gbs_build_keys(const GbsDict& t, const int32_t* slots, const uint64_t* knull, int64_t groups,
+                              char** out_chars, int64_t** out_ends, cudaStream_t s) {
+    *out_chars = nullptr;
+    *out_ends = nullptr;
+    long long *clen = nullptr, *tot = nullptr;
+    int32_t rc = dev_alloc(reinterpret_cast<void**>(&clen), static_cast<size_t>(groups) * 8, s);
+    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&tot), 8, s);
+    long long nchars = 0;
+    if (rc == QDB_OK) {
+        gbs_len_kernel<<<gbs_grid(static_cast<uint64_t>(groups)), 256, 0, s>>>(t, slots, knull, groups, clen);
+        note_launch();
+        rc = exclusive_scan<long long>(clen, groups, tot, s);
+        cudaError_t e = rc == QDB_OK ? cudaMemcpyAsync(&nchars, tot, 8, cudaMemcpyDeviceToHost, s) : cudaSuccess;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (rc == QDB_OK && e != cudaSuccess) rc = cuda_fail(e, "string keys: lengths");
+    }
+    if (rc == QDB_OK)
+        rc = dev_alloc(reinterpret_cast<void**>(out_chars), static_cast<size_t>(std::max<long long>(nchars, 1)), s);
+    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(out_ends), static_cast<size_t>(groups) * 8, s);
+    if (rc == QDB_OK) {
+        gbs_emit_kernel<<<gbs_grid(static_cast<uint64_t>(groups)), 256, 0, s>>>(t, slots, knull, groups, clen,
+                                                                                *out_chars, *out_ends);
+        note_launch();
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "gbs_emit_kernel");
+    }
+    dev_free(clen, s);
+    dev_free(tot, s);
+    if (rc != QDB_OK) {
+        dev_free(*out_chars, s);
+        dev_free(*out_ends, s);
+        *out_chars = nullptr;
+        *out_ends = nullptr;
+    }
+    return rc;
 }
 
 }  // namespace qdb
@@ -390,36 +456,10 @@ int32_t qdb_gbs_results(qdb_gbs* g, int32_t n_aggs, const int32_t* aggs, char** 
         dev_free(knull, s);
         return QDB_OK;
     }
-    long long *clen = nullptr, *tot = nullptr;
-    rc = dev_alloc(reinterpret_cast<void**>(&clen), static_cast<size_t>(groups) * 8, s);
-    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&tot), 8, s);
-    long long nchars = 0;
-    if (rc == QDB_OK) {
-        const unsigned grid = gbs_grid(static_cast<uint64_t>(groups));
-        gbs_len_kernel<<<grid, 256, 0, s>>>(g->t, static_cast<const int32_t*>(slots), knull, groups, clen);
-        note_launch();
-        rc = exclusive_scan<long long>(clen, groups, tot, s);
-        cudaError_t e = rc == QDB_OK ? cudaMemcpyAsync(&nchars, tot, 8, cudaMemcpyDeviceToHost, s) : cudaSuccess;
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (rc == QDB_OK && e != cudaSuccess) rc = cuda_fail(e, "qdb_gbs_results: key lengths");
-    }
-    if (rc == QDB_OK)
-        rc = dev_alloc(reinterpret_cast<void**>(out_chars), static_cast<size_t>(std::max<long long>(nchars, 1)), s);
-    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(out_ends), static_cast<size_t>(groups) * 8, s);
-    if (rc == QDB_OK) {
-        gbs_emit_kernel<<<gbs_grid(static_cast<uint64_t>(groups)), 256, 0, s>>>(
-            g->t, static_cast<const int32_t*>(slots), knull, groups, clen, *out_chars, *out_ends);
-        note_launch();
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) rc = cuda_fail(e, "gbs_emit_kernel");
-    }
-    dev_free(clen, s);
-    dev_free(tot, s);
+    rc = gbs_build_keys(g->t, static_cast<const int32_t*>(slots), knull, groups, out_chars, out_ends, s);
     dev_free(slots, s);
     if (rc != QDB_OK) {
         dev_free(knull, s);
-        dev_free(*out_chars, s);
-        dev_free(*out_ends, s);
         for (int j = 0; j < n_aggs; ++j) {
             dev_free(out_vals[j], s);
             out_vals[j] = nullptr;
@@ -428,14 +468,88 @@ int32_t qdb_gbs_results(qdb_gbs* g, int32_t n_aggs, const int32_t* aggs, char** 
                 out_val_nulls[j] = nullptr;
             }
         }
-        *out_chars = nullptr;
-        *out_ends = nullptr;
         return rc;
     }
     *out_count = groups;
     if (out_key_nulls) *out_key_nulls = knull;
     else dev_free(knull, s);
     return QDB_OK;
+}
+
+int32_t qdb_gbs_export(qdb_gbs* g, char** out_chars, int64_t** out_ends, uint64_t** out_state, uint8_t** out_flags,
+                       int64_t* out_count, void* stream) {
+    if (!g || !out_chars || !out_ends || !out_state || !out_flags || !out_count)
+        return fail(QDB_ERR_INVALID, "qdb_gbs_export: null argument");
+    *out_chars = nullptr;
+    *out_ends = nullptr;
+    *out_count = 0;
+    cudaStream_t s = as_stream(stream);
+    uint64_t* keys = nullptr;
+    int64_t n = 0;
+    int32_t rc = qdb_gb_export_partitioned(g->num, 1, &keys, out_state, out_flags, &n, stream);
+    if (rc != QDB_OK) return rc;
+    int32_t* slots = nullptr;
+    unsigned long long* knull = nullptr;
+    const size_t words = static_cast<size_t>((n + 63) / 64);
+    if (n > 0) {
+        rc = dev_alloc(reinterpret_cast<void**>(&slots), static_cast<size_t>(n) * 4, s);
+        if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&knull), words * 8, s);
+        if (rc == QDB_OK) {
+            cudaError_t e = cudaMemsetAsync(knull, 0, words * 8, s);
+            if (e == cudaSuccess) {
+                gbs_export_prep_kernel<<<gbs_grid(static_cast<uint64_t>(n)), 256, 0, s>>>(keys, *out_flags, n, slots, knull);
+                note_launch();
+                e = cudaGetLastError();
+            }
+            if (e != cudaSuccess) rc = cuda_fail(e, "gbs_export_prep_kernel");
+        }
+        if (rc == QDB_OK) rc = gbs_build_keys(g->t, slots, reinterpret_cast<const uint64_t*>(knull), n, out_chars, out_ends, s);
+    }
+    dev_free(keys, s);
+    dev_free(slots, s);
+    dev_free(knull, s);
+    if (rc != QDB_OK) {
+        dev_free(*out_state, s);
+        dev_free(*out_flags, s);
+        *out_state = nullptr;
+        *out_flags = nullptr;
+        return rc;
+    }
+    *out_count = n;
+    return QDB_OK;
+}
+
+int32_t qdb_gbs_state_words(qdb_gbs* g, int32_t* out_words) {
+    if (!g || !out_words) return fail(QDB_ERR_INVALID, "qdb_gbs_state_words: null argument");
+    return qdb_gb_state_words(g->num, out_words);
+}
+
+int32_t qdb_gbs_merge_exported(qdb_gbs* g, const char* chars, const int64_t* ends, const uint64_t* state,
+                               const uint8_t* flags, int64_t n, void* stream) {
+    if (!g || n < 0 || (n > 0 && (!ends || !flags))) return fail(QDB_ERR_INVALID, "qdb_gbs_merge_exported: bad arguments");
+    if (n == 0) return QDB_OK;
+    cudaStream_t s = as_stream(stream);
+    int8_t* mask = nullptr;
+    int32_t* ids = nullptr;
+    uint64_t* keys = nullptr;
+    int32_t rc = dev_alloc(reinterpret_cast<void**>(&mask), static_cast<size_t>(n), s);
+    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&ids), static_cast<size_t>(n) * 4, s);
+    if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&keys), static_cast<size_t>(n) * 8, s);
+    if (rc == QDB_OK) {
+        const unsigned grid = gbs_grid(static_cast<uint64_t>(n));
+        gbs_merge_prep_kernel<<<grid, 256, 0, s>>>(flags, n, mask);
+        const uintptr_t base = reinterpret_cast<uintptr_t>(chars);
+        gbs_map_kernel<<<grid, kGbsThreads, 0, s>>>(g->t, reinterpret_cast<const uint64_t*>(base & ~uintptr_t(7)),
+                                                    static_cast<int64_t>(base & 7), ends, nullptr, mask, n, ids);
+        gbs_keywords_kernel<<<grid, 256, 0, s>>>(ids, n, keys);
+        note_launch(3);
+        const cudaError_t e = cudaGetLastError();
+        rc = e == cudaSuccess ? qdb_gb_merge_partial(g->num, keys, state, flags, n, stream) : cuda_fail(e, "string merge");
+    }
+    dev_free(mask, s);
+    dev_free(ids, s);
+    dev_free(keys, s);
+    return rc;
 }
 
 }  // extern "C"

@@ -594,6 +594,20 @@ class StringGroupByTable:
                        DeviceBuffer(ovn[i], nullmask_words(n), np.uint64))
         return keys, DeviceBuffer(okn.value, nullmask_words(n), np.uint64), vals, n
 
+    def merge_from(self, other: "StringGroupByTable", stream=None) -> None:
+        """Adds every group of `other` (same aggregates and value type, same device) to this table: the string form
+        of GetResults over several tables (qdb_gbs_export + qdb_gbs_merge_exported)."""
+        oc, oe, ost, ofl = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+        n = C.c_int64()
+        capi.check(capi.lib().qdb_gbs_export(other.handle, C.byref(oc), C.byref(oe), C.byref(ost), C.byref(ofl),
+                                             C.byref(n), _stream(stream)))
+        bufs = [DeviceBuffer(x.value, 1, np.uint8) for x in (oc, oe, ost, ofl)]
+        capi.check(capi.lib().qdb_gbs_merge_exported(self.handle, oc.value, oe.value, ost.value, ofl.value, n.value,
+                                                     _stream(stream)))
+        self.check(stream)
+        for b in bufs:
+            b.free(stream)
+
     def results_host(self, aggs: Optional[Sequence[str]] = None, stream=None) -> dict:
         """{key bytes, or None for the NULL key: {agg: value, or None for a NULL aggregate}}."""
         keys, knull, vals, n = self.results(aggs, stream)

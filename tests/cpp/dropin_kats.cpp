@@ -396,6 +396,103 @@ void string_case(const std::string& name, int32_t blocks) {
     GPUMemory::free(vn);
 }
 
+// "smerge" mode: as "string", with the blocks dealt alternately to two tables that GetResults(..., tables) merges
+// (the multi-GPU GetResults, GPUGroupByString.cuh:565).
+template <typename AGG, typename O>
+void string_merge_case(const std::string& name, int32_t blocks) {
+    std::vector<std::unique_ptr<IGroupBy>> tables;
+    tables.emplace_back(new GPUGroupBy<AGG, O, std::string, int32_t>(8, 1));
+    tables.emplace_back(new GPUGroupBy<AGG, O, std::string, int32_t>(8, 1));
+    for (int32_t b = 0; b < blocks; ++b) {
+        auto& gb = *static_cast<GPUGroupBy<AGG, O, std::string, int32_t>*>(tables[b % 2].get());
+        int32_t rows = 0;
+        std::cin >> rows;
+        std::string chars;
+        std::vector<int64_t> ends;
+        std::vector<int32_t> vals;
+        std::vector<nullmask_t> kn(GPUMemory::CalculateNullMaskSize(rows) + 1, 0), vn(kn.size(), 0);
+        bool any_kn = false, any_vn = false, have_vals = true;
+        for (int32_t r = 0; r < rows; ++r) {
+            std::string k, v;
+            int keep = 1;
+            std::cin >> k >> v >> keep;
+            if (!keep) continue;
+            const size_t i = ends.size();
+            if (k == "N") {
+                kn[i / 64] |= nullmask_t(1) << (i % 64);
+                any_kn = true;
+            } else if (k != "-") {
+                for (size_t c = 0; c + 1 < k.size(); c += 2) chars.push_back(static_cast<char>(std::stoi(k.substr(c, 2), nullptr, 16)));
+            }
+            ends.push_back(static_cast<int64_t>(chars.size()));
+            if (v == "X") have_vals = false;
+            else if (v == "N") {
+                vn[i / 64] |= nullmask_t(1) << (i % 64);
+                any_vn = true;
+                vals.push_back(0);
+            } else {
+                vals.push_back(std::stoi(v));
+            }
+        }
+        const int32_t n = static_cast<int32_t>(ends.size());
+        if (n == 0) continue;
+        cuda_ptr<char> dc(chars.size() + 1);
+        if (!chars.empty()) GPUMemory::copyHostToDevice(dc.get(), chars.data(), chars.size());
+        cuda_ptr<int64_t> de = device_col(ends, 0, n);
+        cuda_ptr<nullmask_t> dkn = device_col(kn, 0, static_cast<int32_t>(kn.size()));
+        cuda_ptr<nullmask_t> dvn = device_col(vn, 0, static_cast<int32_t>(vn.size()));
+        cuda_ptr<int32_t> dv(have_vals ? static_cast<size_t>(n) : 1);
+        if (have_vals) GPUMemory::copyHostToDevice(dv.get(), vals.data(), static_cast<size_t>(n));
+        gb.ProcessBlock(GPUMemory::GPUString{dc.get(), de.get()}, have_vals ? dv.get() : nullptr, n,
+                        any_kn ? dkn.get() : nullptr, any_vn ? dvn.get() : nullptr);
+    }
+    GPUMemory::GPUString keys{nullptr, nullptr};
+    O* vals = nullptr;
+    nullmask_t *kn = nullptr, *vn = nullptr;
+    int32_t g = 0;
+    static_cast<GPUGroupBy<AGG, O, std::string, int32_t>*>(tables[0].get())->GetResults(&keys, &vals, &g, tables, &kn, &vn);
+    std::printf("sresult %s %d\n", name.c_str(), g);
+    if (g > 0) {
+        std::vector<int64_t> ends = to_host(keys.stringIndices, g);
+        std::string chars(static_cast<size_t>(ends[g - 1]), '\0');
+        if (!chars.empty()) GPUMemory::copyDeviceToHost(&chars[0], keys.allChars, chars.size());
+        std::vector<O> hv = to_host(vals, g);
+        std::vector<nullmask_t> hkn = to_host(kn, static_cast<int32_t>(GPUMemory::CalculateNullMaskSize(g)));
+        std::vector<nullmask_t> hvn = to_host(vn, static_cast<int32_t>(GPUMemory::CalculateNullMaskSize(g)));
+        for (int32_t i = 0; i < g; ++i) {
+            const int64_t b0 = i ? ends[i - 1] : 0;
+            std::string key;
+            if ((hkn[i / 64] >> (i % 64)) & 1) key = "N";
+            else if (ends[i] == b0) key = "-";
+            else
+                for (int64_t c = b0; c < ends[i]; ++c) {
+                    char hx[3];
+                    std::snprintf(hx, sizeof(hx), "%02x", static_cast<unsigned char>(chars[static_cast<size_t>(c)]));
+                    key += hx;
+                }
+            if ((hvn[i / 64] >> (i % 64)) & 1) std::printf("%s N\n", key.c_str());
+            else std::printf("%s %lld\n", key.c_str(), static_cast<long long>(hv[i]));
+        }
+    }
+    GPUMemory::free(keys);
+    GPUMemory::free(vals);
+    GPUMemory::free(kn);
+    GPUMemory::free(vn);
+}
+
+int run_string_merge() {
+    std::string tag, name, agg;
+    int32_t blocks = 0;
+    while (std::cin >> tag >> name >> agg >> blocks) {
+        if (agg == "sum") string_merge_case<AggregationFunctions::sum, int32_t>(name, blocks);
+        else if (agg == "min") string_merge_case<AggregationFunctions::min, int32_t>(name, blocks);
+        else if (agg == "max") string_merge_case<AggregationFunctions::max, int32_t>(name, blocks);
+        else if (agg == "avg") string_merge_case<AggregationFunctions::avg, int32_t>(name, blocks);
+        else string_merge_case<AggregationFunctions::count, int64_t>(name, blocks);
+    }
+    return 0;
+}
+
 int run_string() {
     std::string tag, name, agg;
     int32_t blocks = 0;
@@ -461,6 +558,7 @@ int main(int argc, char** argv) {
         if (argc > 1 && std::string(argv[1]) == "scalar") return run_scalar();
         if (argc > 1 && std::string(argv[1]) == "string") return run_string();
         if (argc > 1 && std::string(argv[1]) == "compress") return run_compress();
+        if (argc > 1 && std::string(argv[1]) == "smerge") return run_string_merge();
     } catch (const std::exception& e) {
         std::fprintf(stderr, "error: %s\n", e.what());
         return 2;

@@ -166,20 +166,22 @@ def test_dropin_string_groupby(cuda):
                 kt = "N" if k is None else ("-" if k == "" else k.encode().hex())
                 vt = "X" if vals is None else ("N" if vn is not None and vn[i] else str(int(vals[i])))
                 text += f"{kt} {vt} {1 if mask is None else int(mask[i])}\n"
-    r = subprocess.run([exe, "string"], input=text, capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stderr
-    lines = r.stdout.splitlines()
-    i = 0
-    for c in cases:
-        tag, name, g = lines[i].split()
-        assert tag == "sresult" and name == c["name"]
-        got = {}
-        for line in lines[i + 1:i + 1 + int(g)]:
-            k, v = line.split()
-            key = None if k == "N" else (b"" if k == "-" else bytes.fromhex(k))
-            got[key] = None if v == "N" else int(v)
-        assert got == string_expected(c), (name, got)
-        i += 1 + int(g)
+    # "string": block by block through one table; "smerge": blocks dealt to two tables merged by GetResults(tables)
+    for mode in ("string", "smerge"):
+        r = subprocess.run([exe, mode], input=text, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        lines = r.stdout.splitlines()
+        i = 0
+        for c in cases:
+            tag, name, g = lines[i].split()
+            assert tag == "sresult" and name == c["name"]
+            got = {}
+            for line in lines[i + 1:i + 1 + int(g)]:
+                k, v = line.split()
+                key = None if k == "N" else (b"" if k == "-" else bytes.fromhex(k))
+                got[key] = None if v == "N" else int(v)
+            assert got == string_expected(c), (mode, name, got)
+            i += 1 + int(g)
 
 
 @pytest.mark.gpu

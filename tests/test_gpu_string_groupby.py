@@ -201,3 +201,26 @@ def test_string_groupby_empty_and_reset():
     assert tab.results_host()[b"a"]["sum"] == 2.0
     tab.reset()
     assert tab.results_host() == {}
+
+
+def test_string_tables_merge_like_getresults_over_gpus():
+    """Two tables over the two halves of the rows (NULL keys and NULL values included), merged with
+    qdb_gbs_export + qdb_gbs_merge_exported, equal the oracle over all rows: the per-GPU partial tables that
+    GetResults(..., tables) combines (GPUGroupByString.cuh:565-785)."""
+    rng = np.random.default_rng(17)
+    vocab = _vocab(rng, 3000, 30)
+    n = 200_000
+    keys = [vocab[i] for i in np.minimum(rng.zipf(1.3, n) - 1, len(vocab) - 1)]
+    chars, ends = oracle.pack_strings(keys)
+    vals = rng.integers(-10_000, 10_000, n).astype(np.int64)
+    kn_f = rng.random(n) < 0.02
+    vn_f = rng.random(n) < 0.05
+    half = n // 2
+    ta = StringGroupByTable(AGGS, np.int64, 4096)
+    tb = StringGroupByTable(AGGS, np.int64, 4096)
+    for t, b0, b1 in ((ta, 0, half), (tb, half, n)):
+        c0 = int(ends[b0 - 1]) if b0 else 0
+        t.process(GPUString(_dev(chars[c0:int(ends[b1 - 1])]), _dev(ends[b0:b1] - c0)), _dev(vals[b0:b1]), b1 - b0,
+                  _dev(pack_nullmask(kn_f[b0:b1])), _dev(pack_nullmask(vn_f[b0:b1])))
+    ta.merge_from(tb)
+    _check_against_oracle(ta, chars, ends, vals, pack_nullmask(kn_f), pack_nullmask(vn_f), None, np.int64)
