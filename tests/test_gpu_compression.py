@@ -111,3 +111,29 @@ def test_groupby_over_compressed_keys(cuda, kdt, n):
     g = t.results_numpy(["count"])
     r = oracle.groupby(keys, vals, pred=(p, FilterConditions.less, 0.5, np.float32, None))
     assert int(g["count"].sum()) == 2 * int(r["cnt"].sum())
+
+
+def test_groupby_over_compressed_keys_count_only_and_null_predicate(cuda):
+    """A COUNT-only table (the fast pass without a value column) and a predicate with a NULL mask (the
+    decompress-first path) over an AAFL key block."""
+    from qikkdb_b200 import datagen as dg
+    from qikkdb_b200.groupby import pack_nullmask
+    n = (1 << 20) + 333
+    keys = (dg.zipf_i64(41, 0, n, 50_000, 1.2, map_keys=False) - 25_000).astype(np.int32)
+    blk = AaflBlock.compress(_dev(keys))
+    t = GroupByTable(["count"], np.int32, None, 1 << 16)
+    process_aafl(t, blk, None, None)
+    g = t.results_numpy(["count"])
+    r = oracle.groupby(keys)
+    order = np.argsort(g["keys"][0], kind="stable")
+    assert np.array_equal(g["keys"][0][order].astype(np.int64), r["keys"][0])
+    assert np.array_equal(g["count"][order], r["cnt"])
+
+    vals = dg.uniform_i64(41, 1, n, -(1 << 40), 1 << 40)
+    p = dg.uniform_f32(41, 2, n)
+    pn = np.random.default_rng(41).random(n) < 0.1
+    t2 = GroupByTable(["sum", "count", "max"], np.int32, np.int64, 1 << 16)
+    pred = make_pred(_dev(p), FilterConditions.greater, 0.3, np.float32, _dev(pack_nullmask(pn).view(np.int64)))
+    process_aafl(t2, blk, _dev(vals), pred)
+    _groupby_compare(keys, vals, t2, pred_np=(p, FilterConditions.greater, 0.3, np.float32, pack_nullmask(pn)),
+                     aggs=("sum", "count", "max"))
