@@ -55,7 +55,7 @@ __device__ __forceinline__ void load4(const T* p, T (&o)[4]) {
 // VEC: the value and predicate columns start on 16-byte boundaries, so each thread takes four consecutive rows per
 // step with vector loads (two steps in flight); otherwise four rows strided by the grid per step.
 template <typename VT, typename PT, bool VEC>
-__global__ void __launch_bounds__(kScThreads) scalar_kernel(const VT* __restrict__ vals, const uint64_t* __restrict__ vnull,
+__global__ void __launch_bounds__(kScThreads, 6) scalar_kernel(const VT* __restrict__ vals, const uint64_t* __restrict__ vnull,
                                                             int64_t n, const PT* __restrict__ pcol,
                                                             const uint64_t* __restrict__ pnull, PredInterval pi,
                                                             const int8_t* __restrict__ mask, ScalarState* st) {
