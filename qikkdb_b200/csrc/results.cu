@@ -44,11 +44,16 @@ __device__ __forceinline__ int block_excl_scan(int x, int* total) {
     return excl;
 }
 
+// A chunk's slots are walked warp by warp: warp w of the block takes the kResWarpSlots consecutive slots from
+// chunk start + w kResWarpSlots, 32 at a time (one slot per lane), so every load of the key words is coalesced.
+constexpr int kResWarpSlots = kResChunk / (kResThreads / 32);
+
 __global__ void res_count_kernel(SlotSpace sp, int* chunk_counts) {
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kResChunk + threadIdx.x * kResPerThread;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t wbase = static_cast<uint64_t>(blockIdx.x) * kResChunk + static_cast<uint64_t>(warp) * kResWarpSlots;
     int c = 0;
 #pragma unroll 4
-    for (int i = 0; i < kResPerThread; ++i) c += present(sp, base + i) ? 1 : 0;
+    for (int i = 0; i < kResWarpSlots; i += 32) c += present(sp, wbase + i + lane) ? 1 : 0;
     __shared__ int tot;
     block_excl_scan(c, &tot);
     if (threadIdx.x == 0) chunk_counts[blockIdx.x] = tot;
@@ -162,93 +167,98 @@ __device__ void emit_agg(const EmitArgs& a, const uint64_t* slot, uint64_t cnt, 
     if (isnull) set_bit(o.nulls, pos);
 }
 
+// Writes the result row `pos` of slot v: key columns, key NULL bits and every aggregate.
+__device__ void res_emit_one(const EmitArgs& a, uint64_t v, int64_t pos) {
+    const uint64_t per = a.sp.cap + 2;
+    const uint64_t* slot = slot_at(a.sp, v);
+    const uint64_t kw = slot[0];
+    // Key columns and key NULL bits.
+    if (a.composite) {
+        int32_t k0, k1;
+        bool n0 = false, n1 = false;
+        if (v >= per) {  // composite key with NULL components
+            const uint32_t pat = static_cast<uint32_t>(kw >> 32);
+            const int32_t other = static_cast<int32_t>(kw & 0xffffffffull);
+            n0 = pat & 1u;
+            n1 = pat & 2u;
+            k0 = n0 ? 0 : other;
+            k1 = n1 ? 0 : other;
+        } else if (v == per - 1) {  // the key equal to the empty marker
+            k0 = std::numeric_limits<int32_t>::min();
+            k1 = 0;
+        } else {
+            k0 = static_cast<int32_t>(kw >> 32);
+            k1 = static_cast<int32_t>(kw & 0xffffffffull);
+        }
+        static_cast<int32_t*>(a.keys0)[pos] = k0;
+        static_cast<int32_t*>(a.keys1)[pos] = k1;
+        if (n0) set_bit(a.knull0, pos);
+        if (n1) set_bit(a.knull1, pos);
+    } else {
+        const bool is_null = (v == per - 2);
+        const bool is_escape = (v == per - 1);
+        switch (a.key_type) {
+            case QDB_INT32:
+                static_cast<int32_t*>(a.keys0)[pos] = is_null ? 0 : static_cast<int32_t>(kw);
+                break;
+            case QDB_INT64:
+                static_cast<int64_t*>(a.keys0)[pos] =
+                    is_null ? 0 : (is_escape ? std::numeric_limits<int64_t>::min() : static_cast<int64_t>(kw));
+                break;
+            case QDB_FLOAT: {
+                const uint32_t b = is_null ? 0u : static_cast<uint32_t>(kw);
+                float f;
+                memcpy(&f, &b, 4);
+                static_cast<float*>(a.keys0)[pos] = f;
+                break;
+            }
+            case QDB_DOUBLE: {
+                const uint64_t b = is_null ? 0ull : kw;
+                double d;
+                memcpy(&d, &b, 8);
+                static_cast<double*>(a.keys0)[pos] = d;
+                break;
+            }
+            default: break;
+        }
+        if (is_null) set_bit(a.knull0, pos);
+    }
+    // Aggregates.
+    const uint64_t cnt = (a.L.cnt >= 0) ? slot[a.L.cnt] : 0;
+    for (int k = 0; k < a.n_out; ++k) {
+        const OutAgg& o = a.out[k];
+        if (!o.vals) continue;
+        if (o.agg == QDB_AGG_COUNT) {
+            static_cast<int64_t*>(o.vals)[pos] = static_cast<int64_t>(cnt);
+            continue;
+        }
+        switch (a.vk) {
+            case VK_I32: emit_agg<int32_t>(a, slot, cnt, o, pos); break;
+            case VK_I64: emit_agg<int64_t>(a, slot, cnt, o, pos); break;
+            case VK_F32: emit_agg<float>(a, slot, cnt, o, pos); break;
+            case VK_F64: emit_agg<double>(a, slot, cnt, o, pos); break;
+            default: break;
+        }
+    }
+}
+
 __global__ void res_emit_kernel(EmitArgs a) {
-    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kResChunk + threadIdx.x * kResPerThread;
-    uint32_t pres = 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t wbase = static_cast<uint64_t>(blockIdx.x) * kResChunk + static_cast<uint64_t>(warp) * kResWarpSlots;
+    // the warp's present slots, then its offset in the chunk (an exclusive scan of the warp counts)
     int c = 0;
 #pragma unroll 4
-    for (int i = 0; i < kResPerThread; ++i)
-        if (present(a.sp, base + i)) {
-            pres |= 1u << i;
-            ++c;
-        }
+    for (int i = 0; i < kResWarpSlots; i += 32) c += __popc(__ballot_sync(0xffffffffu, present(a.sp, wbase + i + lane)));
     __shared__ int tot;
-    int64_t pos = a.chunk_offsets[blockIdx.x] + block_excl_scan(c, &tot);
-    const uint64_t per = a.sp.cap + 2;
-    for (int i = 0; i < kResPerThread; ++i) {
-        if (!((pres >> i) & 1u)) continue;
-        const uint64_t v = base + i;
-        const uint64_t* slot = slot_at(a.sp, v);
-        const uint64_t kw = slot[0];
-        // Key columns and key NULL bits.
-        if (a.composite) {
-            int32_t k0, k1;
-            bool n0 = false, n1 = false;
-            if (v >= per) {  // composite key with NULL components
-                const uint32_t pat = static_cast<uint32_t>(kw >> 32);
-                const int32_t other = static_cast<int32_t>(kw & 0xffffffffull);
-                n0 = pat & 1u;
-                n1 = pat & 2u;
-                k0 = n0 ? 0 : other;
-                k1 = n1 ? 0 : other;
-            } else if (v == per - 1) {  // the key equal to the empty marker
-                k0 = std::numeric_limits<int32_t>::min();
-                k1 = 0;
-            } else {
-                k0 = static_cast<int32_t>(kw >> 32);
-                k1 = static_cast<int32_t>(kw & 0xffffffffull);
-            }
-            static_cast<int32_t*>(a.keys0)[pos] = k0;
-            static_cast<int32_t*>(a.keys1)[pos] = k1;
-            if (n0) set_bit(a.knull0, pos);
-            if (n1) set_bit(a.knull1, pos);
-        } else {
-            const bool is_null = (v == per - 2);
-            const bool is_escape = (v == per - 1);
-            switch (a.key_type) {
-                case QDB_INT32:
-                    static_cast<int32_t*>(a.keys0)[pos] = is_null ? 0 : static_cast<int32_t>(kw);
-                    break;
-                case QDB_INT64:
-                    static_cast<int64_t*>(a.keys0)[pos] =
-                        is_null ? 0 : (is_escape ? std::numeric_limits<int64_t>::min() : static_cast<int64_t>(kw));
-                    break;
-                case QDB_FLOAT: {
-                    const uint32_t b = is_null ? 0u : static_cast<uint32_t>(kw);
-                    float f;
-                    memcpy(&f, &b, 4);
-                    static_cast<float*>(a.keys0)[pos] = f;
-                    break;
-                }
-                case QDB_DOUBLE: {
-                    const uint64_t b = is_null ? 0ull : kw;
-                    double d;
-                    memcpy(&d, &b, 8);
-                    static_cast<double*>(a.keys0)[pos] = d;
-                    break;
-                }
-                default: break;
-            }
-            if (is_null) set_bit(a.knull0, pos);
-        }
-        // Aggregates.
-        const uint64_t cnt = (a.L.cnt >= 0) ? slot[a.L.cnt] : 0;
-        for (int k = 0; k < a.n_out; ++k) {
-            const OutAgg& o = a.out[k];
-            if (!o.vals) continue;
-            if (o.agg == QDB_AGG_COUNT) {
-                static_cast<int64_t*>(o.vals)[pos] = static_cast<int64_t>(cnt);
-                continue;
-            }
-            switch (a.vk) {
-                case VK_I32: emit_agg<int32_t>(a, slot, cnt, o, pos); break;
-                case VK_I64: emit_agg<int64_t>(a, slot, cnt, o, pos); break;
-                case VK_F32: emit_agg<float>(a, slot, cnt, o, pos); break;
-                case VK_F64: emit_agg<double>(a, slot, cnt, o, pos); break;
-                default: break;
-            }
-        }
-        ++pos;
+    int64_t pos = a.chunk_offsets[blockIdx.x] + block_excl_scan(lane == 0 ? c : 0, &tot);
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int i = 0; i < kResWarpSlots; i += 32) {
+        const uint64_t v = wbase + i + lane;
+        const bool pr = present(a.sp, v);
+        const unsigned bal = __ballot_sync(0xffffffffu, pr);
+        if (pr) res_emit_one(a, v, pos + __popc(bal & lt));
+        pos += __popc(bal);
     }
 }
 
