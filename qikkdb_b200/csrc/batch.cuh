@@ -16,8 +16,8 @@ constexpr int kBMaxMembers = 8;                     // queries sharing one scan 
 constexpr int kBMaxRowsPerLane = 4;
 constexpr int kBListRows = 256;                     // rows of a stage tile one consumer warp compacts (u16 list)
 constexpr int kBSmemCap = 192 * 1024;              // shared memory per CTA: the rest stays L1 for the probe loads
-constexpr int kBResThreads = 256;
-constexpr int kBResPer = 16;
+constexpr int kBResThreads = 1024;
+constexpr int kBResPer = 8;
 constexpr int kBResChunk = kBResThreads * kBResPer;
 
 // Shared memory of one warp group in queue q: [header | tables ... | stage ring].

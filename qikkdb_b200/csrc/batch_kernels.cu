@@ -844,47 +844,53 @@ __global__ void __launch_bounds__(kBResThreads) gb_batch_results_kernel(const Ba
     const int64_t cap = I.res_cap;
     __shared__ int tot_s;
     int64_t done = 0;
+    // A chunk's slots are walked warp by warp (warp w: kWS consecutive slots, one per lane per step), so the key-word
+    // loads are coalesced; a row's position is the chunk's base, its warp's offset and its rank in the ballot.
+    constexpr int kWS = kBResChunk / (kBResThreads / 32);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
     for (uint64_t c0 = 0; c0 < total; c0 += kBResChunk) {
-        const uint64_t b = c0 + static_cast<uint64_t>(threadIdx.x) * kBResPer;
-        uint32_t pres = 0;
+        const uint64_t wb = c0 + static_cast<uint64_t>(warp) * kWS;
         int c = 0;
 #pragma unroll 4
-        for (int k = 0; k < kBResPer; ++k) {
-            const uint64_t v = b + k;
-            if (v < total && I.main.slots[v * W] != kEmpty) {
-                pres |= 1u << k;
-                ++c;
-            }
+        for (int k = 0; k < kWS; k += 32) {
+            const uint64_t v = wb + k + lane;
+            c += __popc(__ballot_sync(0xffffffffu, v < total && I.main.slots[v * W] != kEmpty));
         }
-        int64_t pos = done + b_block_scan(c, &tot_s);
-        for (int k = 0; k < kBResPer; ++k) {
-            if (!((pres >> k) & 1u)) continue;
-            const uint64_t v = b + k;
-            uint64_t* slot = I.main.slots + v * W;
-            if (pos < cap) {
-                const uint64_t kw = slot[0];
-                int64_t key;
-                if (v == I.main.mask + 2) key = LLONG_MIN;  // the key equal to the empty marker
-                else if (I.kt == 4) key = static_cast<int32_t>(kw);
-                else key = static_cast<int64_t>(kw);
-                res[pos] = static_cast<uint64_t>(key);
-                int col = 0;
-                for (int a = QDB_AGG_MIN; a <= QDB_AGG_COUNT; a <<= 1) {
-                    if (!(I.aggs & a)) continue;
-                    ++col;
-                    res[static_cast<int64_t>(col) * cap + pos] = b_emit(I, slot, a);
+        int64_t pos = done + b_block_scan(lane == 0 ? c : 0, &tot_s);
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        for (int k = 0; k < kWS; k += 32) {
+            const uint64_t v = wb + k + lane;
+            const bool pr = v < total && I.main.slots[v * W] != kEmpty;
+            const unsigned bal = __ballot_sync(0xffffffffu, pr);
+            if (pr) {
+                const int64_t p = pos + __popc(bal & lt);
+                uint64_t* slot = I.main.slots + v * W;
+                if (p < cap) {
+                    const uint64_t kw = slot[0];
+                    int64_t key;
+                    if (v == I.main.mask + 2) key = LLONG_MIN;  // the key equal to the empty marker
+                    else if (I.kt == 4) key = static_cast<int32_t>(kw);
+                    else key = static_cast<int64_t>(kw);
+                    res[p] = static_cast<uint64_t>(key);
+                    int col = 0;
+                    for (int a = QDB_AGG_MIN; a <= QDB_AGG_COUNT; a <<= 1) {
+                        if (!(I.aggs & a)) continue;
+                        ++col;
+                        res[static_cast<int64_t>(col) * cap + p] = b_emit(I, slot, a);
+                    }
+                }
+                // Clean the slot for the next run.
+                slot[0] = kEmpty;
+                for (int w = 1; w < W; ++w) {
+                    uint64_t x = 0;
+                    if (w == L.mn && L.packed) x = kPackedMinMaxInit;
+                    else if (w == L.mn) x = kMinInit64;
+                    else if (w == L.mx) x = kMaxInit64;
+                    slot[w] = x;
                 }
             }
-            ++pos;
-            // Clean the slot for the next run.
-            slot[0] = kEmpty;
-            for (int w = 1; w < W; ++w) {
-                uint64_t x = 0;
-                if (w == L.mn && L.packed) x = kPackedMinMaxInit;
-                else if (w == L.mn) x = kMinInit64;
-                else if (w == L.mx) x = kMaxInit64;
-                slot[w] = x;
-            }
+            pos += __popc(bal);
         }
         done += tot_s;
         __syncthreads();
