@@ -80,6 +80,12 @@ def parse_args():
     ap.add_argument("--served-rows", type=int, default=1 << 30)
     ap.add_argument("--served-queries", type=int, default=128)
     ap.add_argument("--served-batch", type=int, default=32)
+    ap.add_argument("--served-plain-rows", type=int, default=None,
+                    help="served: row count from which a query runs alone through the single-query fast pass "
+                         "(<= 0: off; default: the library's, 2^22)")
+    ap.add_argument("--served-plain-groups", type=int, default=None,
+                    help="served: table capacity from which a query runs alone through the single-query fast pass "
+                         "(<= 0: off, the library's default)")
     return ap.parse_args()
 
 
@@ -1061,7 +1067,8 @@ def served_measure(args, dev, sub: bool = False) -> dict:
     lib = _capi.lib()
     n = args.served_rows
     cols = served_columns(n, dev)
-    srv = Server(max_batch=args.served_batch, in_flight=2, table_budget=40 << 30, result_budget=4 << 30)
+    srv = Server(max_batch=args.served_batch, in_flight=2, table_budget=40 << 30, result_budget=4 << 30,
+                 plain_rows=args.served_plain_rows, plain_groups=args.served_plain_groups)
     n_q = args.served_queries
     # warm-up, then capacity: every query of a closed burst submitted at once
     warm = served_queries(cols, 16, SERVE_SEED + 99)
@@ -1101,6 +1108,9 @@ def served_measure(args, dev, sub: bool = False) -> dict:
             "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
             "config": {"workload": SERVE_WORKLOAD, "rows": n, "queries_per_rate": n_q, "max_batch": args.served_batch,
                        "in_flight_batches": 2, "table_budget_bytes": 40 << 30,
+                       "single_query_route": {
+                           "min_rows": args.served_plain_rows if args.served_plain_rows is not None else 1 << 22,
+                           "min_groups": args.served_plain_groups or 0},
                        "tables": "sized by the server's cardinality estimate (sampled GEE, capped by the modulus)"},
             "value_is": "closed-burst capacity: all queries submitted at t=0, queries / (first arrival to last result)",
             "burst_p50_ms": burst_p50, "burst_p99_ms": burst_p99,

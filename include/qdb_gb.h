@@ -463,7 +463,8 @@ int32_t qdb_gb_plain_run(const qdb_gb_query* queries, int32_t n, int32_t results
  * batches on the GPU (each on its own stream, executed by the batch engine above, so their work overlaps on the
  * device), admits pending queries in arrival order into the next free batch while their hash tables fit the
  * table budget (table_budget_bytes over all batches in flight, split evenly between them) and their results
- * fit the result budget, and on completion copies every query's results to host memory.  A query whose
+ * fit the result budget, and on completion copies every query's results to host memory.  Large queries (see
+ * qdb_server_set_plain_route) take a slot alone through the single-query operators instead.  A query whose
  * max_groups is 0 gets its table sized from a cardinality estimate (a sample of its key column, GEE estimator of
  * Charikar, Chaudhuri, Motwani and Narasayya, PODS 2000, capped by key_mod); a query that reports
  * QDB_HASH_TABLE_FULL is resubmitted with twice the table, like the dispatcher's restart on GPU_HASH_TABLE_FULL
@@ -489,6 +490,7 @@ typedef struct qdb_server_stats {
     int64_t queries_in_batches; /* sum of batch sizes (mean batch size = queries_in_batches / batches) */
     int64_t table_budget_bytes; /* the table budget the server admits against (after the free-HBM cut) */
     int64_t hbm_free_at_create; /* free device memory when the server was created (cudaMemGetInfo) */
+    int64_t plain_queries;      /* queries run alone through the single-query operators (qdb_server_set_plain_route) */
 } qdb_server_stats;
 
 /* table_budget_bytes is cut down to the device memory free at creation less a reserve (an eighth of the free
@@ -504,6 +506,16 @@ int32_t qdb_server_wait(qdb_server* s, uint64_t ticket, int64_t timeout_ms, qdb_
 /* Frees a finished ticket and its host results. */
 int32_t qdb_server_release(qdb_server* s, uint64_t ticket);
 int32_t qdb_server_stats_get(qdb_server* s, qdb_server_stats* out);
+/* Queries of at least min_rows rows, or whose table capacity (given, or the cardinality estimate) is at least
+ * min_groups, skip the batch engine and run alone on a slot through the single-query operators: the key % key_mod
+ * column (qdb_arith_mod, into a buffer the slot keeps), qdb_gb_create, qdb_gb_process with the fused WHERE,
+ * qdb_gb_results_multi, their results converted to the words of qdb_gb_batch_result.  Batching pays for small
+ * queries, whose launch and synchronisation costs it removes; a large query amortises those, and the single-query
+ * fast pass (shared table plus hash-partitioned spill) hashes its rows faster than the batch kernel.  A threshold
+ * <= 0 is off.  The batch engine still takes single-query-path queries' places in arrival order: the oldest pending
+ * query, if it is for the single-query path, takes the next free slot alone.  Defaults: min_rows 2^22, min_groups
+ * off. */
+int32_t qdb_server_set_plain_route(qdb_server* s, int64_t min_rows, int64_t min_groups);
 /* Open-loop driver: submits queries[i] when arrival_ns[i] (ns after the call, non-decreasing) has come, whatever
  * is still in flight, waits for all of them and writes latency_ns[i] = results on host - arrival time (so queueing
  * delay counts) and status[i]; tickets are released.  *wall_ns = first arrival to last completion. */

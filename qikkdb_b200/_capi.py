@@ -109,7 +109,8 @@ class qdb_server_result(C.Structure):
 
 class qdb_server_stats(C.Structure):
     _fields_ = [(f, C.c_int64) for f in ("submitted", "completed", "batches", "retries", "rejected",
-                                         "queries_in_batches", "table_budget_bytes", "hbm_free_at_create")]
+                                         "queries_in_batches", "table_budget_bytes", "hbm_free_at_create",
+                                         "plain_queries")]
 
 
 P = C.c_void_p
@@ -198,6 +199,7 @@ SIGNATURES = [
     ("qdb_server_wait", I32, [P, C.c_uint64, I64, C.POINTER(qdb_server_result)]),
     ("qdb_server_release", I32, [P, C.c_uint64]),
     ("qdb_server_stats_get", I32, [P, C.POINTER(qdb_server_stats)]),
+    ("qdb_server_set_plain_route", I32, [P, I64, I64]),
     ("qdb_server_run_open_loop", I32, [P, C.POINTER(qdb_gb_query), I32, PI64, PI64, C.POINTER(I32), PI64]),
 ]
 

@@ -161,11 +161,28 @@ namespace qdb {
 // GPUBinary<ArithmeticOperations::mod, T, T*, T> before a GROUP BY over it (GPUBinary.cuh:145-166).
 // The remainder uses the multiply-high form of the division by the invariant |m| (mod_signed, qdb_common.cuh);
 // a % m == a % |m| for C++'s truncating division.
-template <typename T>
-__global__ void mod_kernel(const T* __restrict__ in, ModMagic mm, T* __restrict__ out, int64_t n) {
+template <typename T, typename O = T>
+__global__ void mod_kernel(const T* __restrict__ in, ModMagic mm, O* __restrict__ out, int64_t n) {
     for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-        out[i] = static_cast<T>(mod_signed(static_cast<int64_t>(in[i]), mm.d, mm.m, mm.s1, mm.s2));
+        out[i] = static_cast<O>(mod_signed(static_cast<int64_t>(in[i]), mm.d, mm.m, mm.s1, mm.s2));
+}
+
+// key % m of an int64 column into an int32 column, for 0 < |m| <= INT32_MAX: every remainder lies in (-|m|, |m|), so
+// the narrowed column holds the same values in half the bytes (the serving loop's single-query route groups by it).
+int32_t arith_mod_narrow(const int64_t* in, int64_t modulus, int32_t* out, int64_t n, cudaStream_t s) {
+    if (n < 0 || (n > 0 && (!in || !out))) return fail(QDB_ERR_INVALID, "arith_mod_narrow: bad arguments");
+    if (modulus == 0) return fail(QDB_DIVISION_BY_ZERO, "arith_mod_narrow: modulo by zero");
+    if (modulus > INT32_MAX || modulus < -int64_t(INT32_MAX))
+        return fail(QDB_ERR_INVALID, "arith_mod_narrow: modulus out of int32 range");
+    if (n == 0) return QDB_OK;
+    const DeviceInfo& di = device_info();
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>((n + 255) / 256, int64_t(di.sm_count) * 16));
+    const ModMagic mm = mod_magic(static_cast<uint64_t>(modulus < 0 ? -modulus : modulus));
+    mod_kernel<int64_t, int32_t><<<grid, 256, 0, s>>>(in, mm, out, n);
+    note_launch();
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QDB_OK : cuda_fail(e, "mod_kernel(narrow)");
 }
 
 }  // namespace qdb

@@ -159,6 +159,10 @@ static int32_t spill_acquire(int dev, uint64_t rows, int vbytes, int64_t cells, 
         }
     }
     if (A.rows < rows || A.vbytes < vbytes || A.cells < cells) {
+        // grow every dimension to the largest seen, so that calls of different shapes do not reallocate in turn
+        const uint64_t r = std::max<uint64_t>(rows, A.rows);
+        const int64_t nc = std::max<int64_t>(cells, A.cells);
+        const int32_t vb = std::max<int32_t>(vbytes, A.vbytes);
         dev_free(A.keys, s);
         dev_free(A.vals, s);
         dev_free(A.fill, s);
@@ -168,10 +172,9 @@ static int32_t spill_acquire(int dev, uint64_t rows, int vbytes, int64_t cells, 
         A.rows = 0;
         A.cells = 0;
         A.vbytes = 0;
-        const uint64_t r = std::max<uint64_t>(rows, A.rows);
-        int32_t rc = dev_alloc(reinterpret_cast<void**>(&A.fill), static_cast<size_t>(cells) * sizeof(uint32_t), s);
+        int32_t rc = dev_alloc(reinterpret_cast<void**>(&A.fill), static_cast<size_t>(nc) * sizeof(uint32_t), s);
         if (rc == QDB_OK) rc = dev_alloc(reinterpret_cast<void**>(&A.keys), r * 8, s);
-        if (rc == QDB_OK && vbytes) rc = dev_alloc(&A.vals, r * static_cast<uint64_t>(vbytes), s);
+        if (rc == QDB_OK && vb) rc = dev_alloc(&A.vals, r * static_cast<uint64_t>(vb), s);
         if (rc != QDB_OK) {
             dev_free(A.keys, s);
             dev_free(A.vals, s);
@@ -183,8 +186,8 @@ static int32_t spill_acquire(int dev, uint64_t rows, int vbytes, int64_t cells, 
             return rc;
         }
         A.rows = r;
-        A.cells = cells;
-        A.vbytes = vbytes;
+        A.cells = nc;
+        A.vbytes = vb;
     }
     *out = &A;
     return QDB_OK;

@@ -3,7 +3,8 @@
 // per GPU.  Queries are submitted from any thread; one scheduler thread keeps up to `in_flight` batches on the GPU
 // (one CUDA stream each, so a new batch's kernels start as the previous batch's last CTAs drain), admits pending
 // queries in arrival order against the table and result budgets, reads back results, and resubmits queries whose
-// table overflowed with twice the capacity.
+// table overflowed with twice the capacity.  Large queries (2^22 rows and up by default) skip the batch engine and
+// take a slot alone through the single-query operators, whose fast pass hashes their rows faster.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -20,10 +21,19 @@
 
 namespace qdb {
 
+int32_t arith_mod_narrow(const int64_t* in, int64_t modulus, int32_t* out, int64_t n, cudaStream_t s);
+
 static int64_t now_ns() {
     return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
         .count();
 }
+
+// Queries of at least this many rows run alone through the single-query fast pass instead of a batch: the batch
+// engine removes per-query launch and synchronisation costs, which such a query amortises, and its kernel hashes a
+// row more slowly than the fast pass (shared table plus hash-partitioned spill).  A table-capacity threshold can
+// route queries by their groups as well; it is off by default.
+constexpr int64_t kServerPlainRows = int64_t(1) << 22;
+constexpr int64_t kServerPlainGroups = 0;
 
 struct Ticket {
     qdb_gb_query q{};
@@ -47,6 +57,12 @@ struct Slot {
     int32_t* h_status = nullptr;
     int64_t* h_res = nullptr;
     int64_t h_res_bytes = 0;
+    // a query routed through the single-query operators (one per slot): its table and key % m column
+    bool plain = false;
+    qdb_gb* gb = nullptr;
+    int32_t gb_key_type = 0;      // the table's key type: INT32 for an int64 key % m narrowed to int32
+    void* modcol = nullptr;       // kept across queries, grown on demand
+    int64_t modcol_bytes = 0;
 };
 
 // Sample of a key column (strided rows) kept per column for the cardinality estimates.
@@ -63,6 +79,8 @@ struct qdb_server {
     int32_t in_flight = 0;
     int64_t slot_table_bytes = 0;
     int64_t slot_result_bytes = 0;
+    int64_t plain_rows = qdb::kServerPlainRows;
+    int64_t plain_groups = qdb::kServerPlainGroups;
     std::mutex mu;
     std::condition_variable cv_work;
     std::condition_variable cv_done;
@@ -212,6 +230,180 @@ static void complete_slot(qdb_server* sv, Slot& sl) {
     sv->cv_done.notify_all();
 }
 
+// The aggregate columns of a query in result order (MIN, MAX, SUM, AVG, COUNT).
+static int32_t result_aggs(int32_t mask, int32_t* aggs) {
+    static const int32_t kOrder[5] = {QDB_AGG_MIN, QDB_AGG_MAX, QDB_AGG_SUM, QDB_AGG_AVG, QDB_AGG_COUNT};
+    int32_t na = 0;
+    for (int32_t b : kOrder)
+        if (mask & b) aggs[na++] = b;
+    return na;
+}
+
+static void release_plain(Slot& sl) {
+    if (sl.gb) qdb_gb_destroy(sl.gb);
+    sl.gb = nullptr;
+    sl.plain = false;
+}
+
+// Launches one query on a free slot through the single-query operators, as the dispatcher runs it: the key % m
+// column (GPUBinary modulo), a table of the query's capacity, ProcessBlock with the fused WHERE, completion event.
+static void launch_plain(qdb_server* sv, Slot& sl, uint64_t id) {
+    Ticket* tk;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        tk = sv->tickets[id];
+        tk->start_ns = now_ns();
+        tk->batch_size = 1;
+        sv->stats.plain_queries += 1;
+    }
+    sl.ids.assign(1, id);
+    sl.busy = true;
+    sl.plain = true;
+    const qdb_gb_query& q = tk->q;
+    const void* key = q.keys;
+    int32_t rc = QDB_OK;
+    // an int64 key % m with m <= INT32_MAX groups by an int32 column of the same values
+    const bool narrow = q.key_type == QDB_INT64 && q.key_mod > 0 && q.key_mod <= INT32_MAX;
+    sl.gb_key_type = narrow ? QDB_INT32 : q.key_type;
+    if (q.key_mod > 0 && q.n_rows > 0) {
+        const int64_t bytes = q.n_rows * type_size(sl.gb_key_type);
+        if (bytes > sl.modcol_bytes) {
+            qdb_free(sl.modcol, sl.s);
+            sl.modcol = nullptr;
+            sl.modcol_bytes = 0;
+            rc = qdb_malloc(&sl.modcol, bytes, sl.s);
+            if (rc == QDB_OK) sl.modcol_bytes = bytes;
+        }
+        if (rc == QDB_OK) {
+            if (narrow)
+                rc = arith_mod_narrow(static_cast<const int64_t*>(q.keys), q.key_mod, static_cast<int32_t*>(sl.modcol),
+                                      q.n_rows, sl.s);
+            else
+                rc = qdb_arith_mod(q.key_type, q.keys, q.key_mod, sl.modcol, q.n_rows, sl.s);
+        }
+        key = sl.modcol;
+    }
+    if (rc == QDB_OK)
+        rc = qdb_gb_create(&sl.gb, q.agg_mask, sl.gb_key_type, 1, q.val_type, q.max_groups, QDB_PLACE_AUTO, sl.s);
+    if (rc == QDB_OK && q.n_rows > 0) {
+        const void* kc[1] = {key};
+        rc = qdb_gb_process(sl.gb, kc, nullptr, q.val_type ? q.vals : nullptr, nullptr, q.n_rows,
+                            q.pred.col ? &q.pred : nullptr, nullptr, sl.s);
+    }
+    if (rc == QDB_OK && cudaEventRecord(sl.ev, sl.s) != cudaSuccess) rc = QDB_ERR_CUDA;
+    if (rc != QDB_OK) {
+        cudaStreamSynchronize(sl.s);
+        release_plain(sl);
+        fail_slot_queries(sv, sl, rc);
+    }
+}
+
+// Reads a plain query's results (GetResults) into the server's result layout: keys as int64, integer aggregates
+// sign-extended to int64, float aggregates widened to double, COUNT as int64 -- the words the batch engine emits.
+static int32_t read_plain_results(Slot& sl, Ticket* t) {
+    const qdb_gb_query& q = t->q;
+    int32_t aggs[5];
+    const int32_t na = result_aggs(q.agg_mask, aggs);
+    void* okeys[1] = {nullptr};
+    void* ovals[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int64_t g = 0;
+    int32_t rc = qdb_gb_results_multi(sl.gb, na, aggs, okeys, nullptr, ovals, nullptr, &g, sl.s);
+    const int ks = type_size(sl.gb_key_type);
+    const int vs = q.val_type ? type_size(q.val_type) : 8;
+    // raw columns to the slot's pinned buffer (g <= max_groups, so they fit the result budget the query was admitted
+    // against: at most 8 bytes per word of max_groups + 2 rows)
+    int64_t off[6] = {0, 0, 0, 0, 0, 0};
+    int64_t need = static_cast<int64_t>(g) * ks;
+    for (int32_t j = 0; j < na; ++j) {
+        off[j + 1] = (need + 15) / 16 * 16;
+        need = off[j + 1] + g * (aggs[j] == QDB_AGG_COUNT ? 8 : vs);
+    }
+    if (rc == QDB_OK && need > sl.h_res_bytes) rc = fail(QDB_ERR_TOO_LARGE, "server: plain results exceed the slot's buffer");
+    unsigned char* h = reinterpret_cast<unsigned char*>(sl.h_res);
+    if (rc == QDB_OK && g > 0) {
+        if (cudaMemcpyAsync(h, okeys[0], static_cast<size_t>(g) * ks, cudaMemcpyDeviceToHost, sl.s) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "server: plain keys to host");
+        for (int32_t j = 0; j < na && rc == QDB_OK; ++j) {
+            const int w = aggs[j] == QDB_AGG_COUNT ? 8 : vs;
+            if (cudaMemcpyAsync(h + off[j + 1], ovals[j], static_cast<size_t>(g) * w, cudaMemcpyDeviceToHost,
+                                sl.s) != cudaSuccess)
+                rc = cuda_fail(cudaGetLastError(), "server: plain results to host");
+        }
+        if (rc == QDB_OK && cudaStreamSynchronize(sl.s) != cudaSuccess)
+            rc = cuda_fail(cudaGetLastError(), "server: plain results");
+    }
+    qdb_free(okeys[0], sl.s);
+    for (void* v : ovals) qdb_free(v, sl.s);
+    if (rc != QDB_OK) return rc;
+    t->n_groups = g;
+    t->n_cols = na;
+    t->data.resize(static_cast<size_t>(g) * (1 + na));
+    int64_t* d = t->data.data();
+    for (int64_t i = 0; i < g; ++i) {
+        if (ks == 4) {
+            int32_t k;
+            memcpy(&k, h + i * 4, 4);
+            d[i] = k;
+        } else {
+            memcpy(&d[i], h + i * 8, 8);
+        }
+    }
+    for (int32_t j = 0; j < na; ++j) {
+        const unsigned char* src = h + off[j + 1];
+        int64_t* dst = d + static_cast<size_t>(g) * (j + 1);
+        if (aggs[j] == QDB_AGG_COUNT || q.val_type == QDB_INT64 || q.val_type == QDB_DOUBLE) {
+            memcpy(dst, src, static_cast<size_t>(g) * 8);
+        } else if (q.val_type == QDB_INT32) {
+            for (int64_t i = 0; i < g; ++i) {
+                int32_t v;
+                memcpy(&v, src + i * 4, 4);
+                dst[i] = v;
+            }
+        } else {  // QDB_FLOAT
+            for (int64_t i = 0; i < g; ++i) {
+                float f;
+                memcpy(&f, src + i * 4, 4);
+                const double x = static_cast<double>(f);
+                memcpy(&dst[i], &x, 8);
+            }
+        }
+    }
+    return QDB_OK;
+}
+
+// A plain query finished: its results to the ticket, or a resubmission with twice the table after HASH_TABLE_FULL.
+static void complete_plain(qdb_server* sv, Slot& sl) {
+    Ticket* t;
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        t = sv->tickets[sl.ids[0]];
+    }
+    int32_t st = qdb_gb_check(sl.gb, sl.s);
+    bool retry = false;
+    if (st == QDB_HASH_TABLE_FULL && t->retries < 16 && t->q.max_groups < (int64_t(1) << 30)) {
+        t->q.max_groups = std::min<int64_t>(t->q.max_groups * 2, int64_t(1) << 30);
+        t->retries += 1;
+        retry = true;
+    } else if (st == QDB_OK) {
+        st = read_plain_results(sl, t);
+    }
+    release_plain(sl);
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (retry) {
+        sv->pending.push_front(sl.ids[0]);
+        sv->stats.retries += 1;
+    } else {
+        if (st != QDB_OK) {
+            t->n_groups = 0;
+            t->data.clear();
+        }
+        finish_ticket(sv, t, st);
+    }
+    sl.ids.clear();
+    sl.busy = false;
+    sv->cv_done.notify_all();
+}
+
 static void scheduler(qdb_server* sv) {
     cudaSetDevice(sv->device);
     for (;;) {
@@ -221,10 +413,12 @@ static void scheduler(qdb_server* sv) {
             if (!sl.busy) continue;
             const cudaError_t e = cudaEventQuery(sl.ev);
             if (e == cudaSuccess) {
-                complete_slot(sv, sl);
+                if (sl.plain) complete_plain(sv, sl);
+                else complete_slot(sv, sl);
                 progressed = true;
             } else if (e != cudaErrorNotReady) {
                 cudaGetLastError();
+                if (sl.plain) release_plain(sl);
                 fail_slot_queries(sv, sl, QDB_ERR_CUDA);
                 progressed = true;
             }
@@ -249,30 +443,48 @@ static void scheduler(qdb_server* sv) {
                 std::lock_guard<std::mutex> lock(sv->mu);
                 t->q.max_groups = est;
             }
+            uint64_t plain_id = 0;
             {
                 std::lock_guard<std::mutex> lock(sv->mu);
                 int64_t tb = 0, rb = 0;
-                while (!sv->pending.empty() && static_cast<int32_t>(ids.size()) < sv->max_batch) {
-                    const uint64_t id = sv->pending.front();
+                // Pending queries in arrival order: the oldest, if it is for the single-query path, takes this slot
+                // alone; otherwise the batch takes batch-path queries in order and passes over single-query ones,
+                // which stay pending for the next free slot (so they do not cut the batch's shared scans short).
+                auto it = sv->pending.begin();
+                while (it != sv->pending.end() && static_cast<int32_t>(ids.size()) < sv->max_batch) {
+                    const uint64_t id = *it;
                     Ticket* t = sv->tickets[id];
                     if (t->q.max_groups <= 0) break;  // arrived after this round's estimates: next round
                     int64_t qt = 0, qr = 0;
                     if (qdb_gb_batch_required(&t->q, 1, &qt, &qr) != QDB_OK || qt > sv->slot_table_bytes ||
                         qr > sv->slot_result_bytes) {
-                        sv->pending.pop_front();
+                        it = sv->pending.erase(it);
                         sv->stats.rejected += 1;
                         finish_ticket(sv, t, QDB_ERR_TOO_LARGE);
                         sv->cv_done.notify_all();
+                        continue;
+                    }
+                    if ((sv->plain_rows > 0 && t->q.n_rows >= sv->plain_rows) ||
+                        (sv->plain_groups > 0 && t->q.max_groups >= sv->plain_groups)) {
+                        if (ids.empty() && it == sv->pending.begin()) {
+                            plain_id = id;
+                            sv->pending.pop_front();
+                            break;
+                        }
+                        ++it;
                         continue;
                     }
                     if (tb + qt > sv->slot_table_bytes || rb + qr > sv->slot_result_bytes) break;
                     tb += qt;
                     rb += qr;
                     ids.push_back(id);
-                    sv->pending.pop_front();
+                    it = sv->pending.erase(it);
                 }
             }
-            if (!ids.empty()) {
+            if (plain_id != 0) {
+                launch_plain(sv, sl, plain_id);
+                progressed = true;
+            } else if (!ids.empty()) {
                 launch_slot(sv, sl, ids);
                 progressed = true;
             }
@@ -374,6 +586,8 @@ int32_t qdb_server_destroy(qdb_server* sv) {
     for (Slot& sl : sv->slots) {
         if (sl.s) cudaStreamSynchronize(sl.s);
         qdb_gb_batch_destroy(sl.b);
+        if (sl.gb) qdb_gb_destroy(sl.gb);
+        qdb_free(sl.modcol, sl.s);
         if (sl.ev) cudaEventDestroy(sl.ev);
         if (sl.s) cudaStreamDestroy(sl.s);
         if (sl.h_counts) cudaFreeHost(sl.h_counts);
@@ -432,6 +646,14 @@ int32_t qdb_server_release(qdb_server* sv, uint64_t ticket) {
     if (!it->second->done) return fail(QDB_ERR_INVALID, "qdb_server_release: query still running");
     delete it->second;
     sv->tickets.erase(it);
+    return QDB_OK;
+}
+
+int32_t qdb_server_set_plain_route(qdb_server* sv, int64_t min_rows, int64_t min_groups) {
+    if (!sv) return fail(QDB_ERR_INVALID, "qdb_server_set_plain_route: null server");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->plain_rows = min_rows;
+    sv->plain_groups = min_groups;
     return QDB_OK;
 }
 

@@ -21,12 +21,18 @@ from .groupby import CODE_TO_NP, type_code
 
 class Server:
     def __init__(self, max_batch: int = 32, in_flight: int = 2, table_budget: int = 1 << 32,
-                 result_budget: int = 1 << 30):
+                 result_budget: int = 1 << 30, plain_rows: int | None = None, plain_groups: int | None = None):
+        """plain_rows / plain_groups: queries of at least plain_rows rows, or whose table capacity is at least
+        plain_groups, run alone through the single-query fast pass (qdb_server_set_plain_route; <= 0 is off; None
+        keeps the library's default: 2^22 rows, groups off)."""
         h = C.c_void_p()
         capi.check(capi.lib().qdb_server_create(C.byref(h), int(max_batch), int(in_flight), int(table_budget),
                                                 int(result_budget)))
         self.handle = h
         self._alive: dict[int, Query] = {}
+        if plain_rows is not None or plain_groups is not None:
+            capi.check(capi.lib().qdb_server_set_plain_route(
+                h, int(1 << 22 if plain_rows is None else plain_rows), int(plain_groups or 0)))
 
     def close(self) -> None:
         if getattr(self, "handle", None) and self.handle.value:

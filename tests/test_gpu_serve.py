@@ -25,7 +25,7 @@ N = 1 << 20
 def columns(cuda):
     h = {"k32": dg.uniform_i32(500, 0, N, 0, (1 << 31) - 1), "k64": dg.uniform_i64(500, 1, N, 0, 1 << 62),
          "p": dg.uniform_f32(500, 2, N), "v": dg.lognormal_f32(500, 3, N, 2.0, 1.0),
-         "vi": dg.uniform_i64(500, 4, N, -(1 << 40), 1 << 40)}
+         "vi": dg.uniform_i64(500, 4, N, -(1 << 40), 1 << 40), "v32": dg.uniform_i32(500, 5, N, -(1 << 20), 1 << 20)}
     d = {k: torch.from_numpy(a).cuda() for k, a in h.items()}
     return h, d
 
@@ -34,12 +34,12 @@ SHAPES = [("k32", "v", ["sum", "min", "max", "count"]), ("k64", "v", ["sum", "av
           ("k64", "vi", ["sum", "count", "max"]), ("k32", "vi", list(AGG_ORDER))]
 
 
-def make_queries(cols, n_q, seed, max_groups_known=False):
+def make_queries(cols, n_q, seed, max_groups_known=False, shapes=SHAPES):
     h, d = cols
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n_q):
-        kc, vc, aggs = SHAPES[i % len(SHAPES)]
+        kc, vc, aggs = shapes[i % len(shapes)]
         card = int(np.exp(rng.uniform(np.log(10), np.log(200_000))))
         sel = float(np.float32(rng.uniform(0.01, 1.0)))
         ek = np.fmod(h[kc], card)
@@ -143,4 +143,55 @@ def test_server_open_loop(columns):
     lat, st, wall = srv.run_open_loop([q for q, _, _ in qs], poisson_arrivals(2000.0, len(qs), 7))
     assert (st == 0).all() and (lat > 0).all() and wall > 0
     assert srv.stats()["completed"] == len(qs)
+    srv.close()
+
+
+PLAIN_SHAPES = SHAPES + [("k64", "v32", list(AGG_ORDER)), ("k32", "v", list(AGG_ORDER))]
+
+
+@pytest.mark.parametrize("route", [{"plain_rows": 1}, {"plain_rows": 0, "plain_groups": 50_000}])
+def test_server_plain_route_matches_oracle(columns, route):
+    """Queries routed through the single-query fast pass (every query by its row count, or those whose estimated
+    tables reach 50K groups) give the oracle's results in the server's result words: int32 and int64 keys, int32 /
+    int64 / float aggregates of every kind."""
+    qs = make_queries(columns, 18, 11, shapes=PLAIN_SHAPES)
+    srv = Server(max_batch=6, in_flight=2, table_budget=1 << 30, result_budget=1 << 28, **route)
+    tickets = [srv.submit(q) for q, _, _ in qs]
+    for (q, ref, vf), t in zip(qs, tickets):
+        r = srv.wait(t)
+        assert r["status"] == 0
+        check(r, ref, q.aggs, vf)
+    st = srv.stats()
+    assert st["completed"] == len(qs)
+    if route.get("plain_rows") == 1:
+        assert st["plain_queries"] == len(qs) and st["batches"] == 0
+    else:
+        assert 0 < st["plain_queries"] < len(qs) and st["batches"] > 0
+    srv.close()
+
+
+def test_server_plain_route_off_batches_everything(columns):
+    qs = make_queries(columns, 8, 12)
+    srv = Server(max_batch=8, in_flight=2, table_budget=1 << 30, result_budget=1 << 28, plain_rows=0, plain_groups=0)
+    for (q, ref, vf), t in zip(qs, [srv.submit(q) for q, _, _ in qs]):
+        r = srv.wait(t)
+        assert r["status"] == 0
+        check(r, ref, q.aggs, vf)
+    assert srv.stats()["plain_queries"] == 0
+    srv.close()
+
+
+def test_server_plain_route_retries_when_table_overflows(columns):
+    """A plain-routed query whose table is far too small reports HASH_TABLE_FULL from the fast pass and is resubmitted
+    with twice the table until it fits."""
+    h, d = columns
+    card = 70_000
+    ek = np.fmod(h["k64"], card)
+    q = Query(d["k64"], d["v32"], ["min", "sum", "count"], 1000, key_mod=card)
+    ref = oracle.groupby(ek, h["v32"])
+    srv = Server(max_batch=4, in_flight=2, table_budget=1 << 30, result_budget=1 << 28, plain_groups=1)
+    r = srv.wait(srv.submit(q))
+    assert r["status"] == 0 and r["retries"] >= 1 and r["max_groups"] >= card
+    check(r, ref, q.aggs, False)
+    assert srv.stats()["plain_queries"] == 1 + r["retries"]
     srv.close()
