@@ -41,3 +41,19 @@ def test_mod_by_zero(cuda):
     with pytest.raises(capi.QdbError) as e:
         _mod(a, 0)
     assert e.value.code == capi.QDB_DIVISION_BY_ZERO
+
+
+@pytest.mark.parametrize("dt", [np.int32, np.int64])
+@pytest.mark.parametrize("n,off", [(1, 0), (3, 0), (5, 0), (4097, 0), ((1 << 20) + 3, 0), (4099, 1), (4099, 3)])
+def test_mod_ragged_and_unaligned(cuda, dt, n, off):
+    """Row counts that leave 1-3 rows after the 4-row vector steps, and columns starting off a 16-byte boundary
+    (the scalar form), against numpy's fmod."""
+    a = (dg.uniform_i32(602, 0, n + off, -(2**31), 2**31 - 1) if dt == np.int32
+         else dg.uniform_i64(602, 0, n + off, -(2**63), 2**63 - 1))
+    d = torch.from_numpy(a).cuda()[off:]
+    out = torch.full((n + off,), 7, dtype=d.dtype, device="cuda")[off:]
+    code = capi.QDB_INT32 if dt == np.int32 else capi.QDB_INT64
+    for m in (3, 1000, -77):
+        capi.check(capi.lib().qdb_arith_mod(code, d.data_ptr(), m, out.data_ptr(), n,
+                                            torch.cuda.current_stream().cuda_stream))
+        assert (out.cpu().numpy() == np.fmod(a[off:], dt(m))).all(), (n, off, m)
