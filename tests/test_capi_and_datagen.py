@@ -72,3 +72,18 @@ def test_generator_distributions():
     assert lu.min() >= 1000 and lu.max() <= 4_000_000
     keys = dg.zipf_i64(1, 5, 1000, 100, 1.1)
     assert (keys != np.iinfo(np.int64).min).all()
+
+
+def test_server_entry_points_reject_null_handles_without_gpu():
+    """The serving loop's entry points check their arguments before any CUDA call: a null server is
+    QDB_ERR_INVALID with a message, on a machine without a GPU too."""
+    import ctypes
+    lib = _capi.lib()
+    st = _capi.qdb_server_stats()
+    assert lib.qdb_server_set_plain_route(None, 1 << 22, 0) == _capi.QDB_ERR_INVALID
+    assert b"qdb_server_set_plain_route" in lib.qdb_last_error()
+    assert lib.qdb_server_stats_get(None, ctypes.byref(st)) == _capi.QDB_ERR_INVALID
+    t = ctypes.c_uint64()
+    assert lib.qdb_server_submit(None, None, ctypes.byref(t)) == _capi.QDB_ERR_INVALID
+    assert lib.qdb_server_release(None, 1) == _capi.QDB_ERR_INVALID
+    assert lib.qdb_server_destroy(None) == 0
