@@ -201,6 +201,15 @@ int32_t qdb_aafl_compress(int32_t type, const void* in, int64_t rows, int64_t mi
  * a malformed block latches QDB_ERR_INVALID for qdb_gb_check. */
 int32_t qdb_gb_process_aafl(qdb_gb* gb, const qdb_aafl_col* keys, const void* vals, const qdb_pred* pred,
                             void* stream);
+/* ProcessBlock of the expression key % key_mod (C++ remainder) of a single INT32 or INT64 key column: the
+ * dispatcher's GPUBinary<ArithmeticOperations::mod> column (GPUBinary.cuh:145-166) followed by ProcessBlock
+ * (GPUGroupBy.cuh:395-410), fused -- the fast pass takes each key's remainder (multiply-high by the invariant |m|) as
+ * it reads the key, so no remainder column is written or read.  Where the fast pass does not apply (fewer than 2048
+ * rows, unaligned columns, a table placed QDB_PLACE_GLOBAL) the remainder column is materialised first.  `vals` and
+ * `pred` as in qdb_gb_process, no NULL masks; key_mod must fit the key type (QDB_DIVISION_BY_ZERO for 0).
+ * Asynchronous like qdb_gb_process. */
+int32_t qdb_gb_process_mod(qdb_gb* gb, const void* keys, int64_t key_mod, const void* vals, const qdb_pred* pred,
+                           int64_t n, void* stream);
 /* Synchronises `stream`, returns and clears the latched kernel status (QDB_OK or QDB_HASH_TABLE_FULL). */
 int32_t qdb_gb_check(qdb_gb* gb, void* stream);
 /* ProcessBlock followed by the Swap check: the synchronous form the reference exposes. */
@@ -507,8 +516,8 @@ int32_t qdb_server_wait(qdb_server* s, uint64_t ticket, int64_t timeout_ms, qdb_
 int32_t qdb_server_release(qdb_server* s, uint64_t ticket);
 int32_t qdb_server_stats_get(qdb_server* s, qdb_server_stats* out);
 /* Queries of at least min_rows rows, or whose table capacity (given, or the cardinality estimate) is at least
- * min_groups, skip the batch engine and run alone on a slot through the single-query operators: the key % key_mod
- * column (qdb_arith_mod, into a buffer the slot keeps), qdb_gb_create, qdb_gb_process with the fused WHERE,
+ * min_groups, skip the batch engine and run alone on a slot through the single-query operators: qdb_gb_create,
+ * qdb_gb_process_mod (key % key_mod fused into the pass) or qdb_gb_process, with the fused WHERE, then
  * qdb_gb_results_multi, their results converted to the words of qdb_gb_batch_result.  Batching pays for small
  * queries, whose launch and synchronisation costs it removes; a large query amortises those, and the single-query
  * fast pass (shared table plus hash-partitioned spill) hashes its rows faster than the batch kernel.  A threshold

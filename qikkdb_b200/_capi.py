@@ -192,6 +192,7 @@ SIGNATURES = [
     ("qdb_aafl_decompress", I32, [C.POINTER(qdb_aafl_col), P, P]),
     ("qdb_aafl_compress", I32, [I32, P, I64, I64, I64, PP, C.POINTER(I64), P]),
     ("qdb_gb_process_aafl", I32, [P, C.POINTER(qdb_aafl_col), P, C.POINTER(qdb_pred), P]),
+    ("qdb_gb_process_mod", I32, [P, P, I64, P, C.POINTER(qdb_pred), I64, P]),
     ("qdb_pred_block_may_pass", I32, [C.POINTER(qdb_pred), P, P, C.POINTER(I32)]),
     ("qdb_server_create", I32, [PP, I32, I32, I64, I64]),
     ("qdb_server_destroy", I32, [P]),

@@ -28,7 +28,7 @@ NVCC_FLAGS = [
 CUDA_SOURCES = [
     "runtime.cu", "groupby.cu", "results.cu", "exchange.cu", "filter.cu", "reconstruct.cu", "hostpipe.cu",
     "agg_i32.cu", "agg_i64.cu", "agg_f32.cu", "agg_f64.cu", "agg_comp.cu", "fast_i32.cu", "fast_i64.cu", "fast_f32.cu",
-    "fast_f64.cu", "fast_comp.cu", "batch.cu", "batch_kernels.cu",
+    "fast_f64.cu", "fast_comp.cu", "fast_i32_mod.cu", "fast_i64_mod.cu", "batch.cu", "batch_kernels.cu",
     "serve.cu", "orderby.cu", "scalar.cu", "groupby_string.cu", "compression.cu",
 ]
 EXTRA_CUDA_SOURCES: list[str] = []

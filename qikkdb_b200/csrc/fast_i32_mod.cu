@@ -1,0 +1,8 @@
+// Fast aggregation pass instantiations for int32_t keys grouped by key % m (the remainder taken as the keys are read).
+#include "groupby_fast.cuh"
+
+namespace qdb {
+int32_t launch_fast_i32_mod(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st) {
+    return launch_fast_k<int32_t, false, true>(a, vk, ptype, smem, st);
+}
+}  // namespace qdb

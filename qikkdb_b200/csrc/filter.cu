@@ -226,18 +226,6 @@ static int32_t launch_mod(const T* in, const ModMagic& mm, O* out, int64_t n, cu
     return e == cudaSuccess ? QDB_OK : cuda_fail(e, "mod_kernel");
 }
 
-// key % m of an int64 column into an int32 column, for 0 < |m| <= INT32_MAX: every remainder lies in (-|m|, |m|), so
-// the narrowed column holds the same values in half the bytes (the serving loop's single-query route groups by it).
-int32_t arith_mod_narrow(const int64_t* in, int64_t modulus, int32_t* out, int64_t n, cudaStream_t s) {
-    if (n < 0 || (n > 0 && (!in || !out))) return fail(QDB_ERR_INVALID, "arith_mod_narrow: bad arguments");
-    if (modulus == 0) return fail(QDB_DIVISION_BY_ZERO, "arith_mod_narrow: modulo by zero");
-    if (modulus > INT32_MAX || modulus < -int64_t(INT32_MAX))
-        return fail(QDB_ERR_INVALID, "arith_mod_narrow: modulus out of int32 range");
-    if (n == 0) return QDB_OK;
-    const ModMagic mm = mod_magic(static_cast<uint64_t>(modulus < 0 ? -modulus : modulus));
-    return launch_mod<int64_t, int32_t>(in, mm, out, n, s);
-}
-
 }  // namespace qdb
 
 extern "C" int32_t qdb_arith_mod(int32_t type, const void* in, int64_t modulus, void* out, int64_t n, void* stream) {

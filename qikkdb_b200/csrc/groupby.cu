@@ -100,6 +100,11 @@ static int32_t launch_spill(const qdb_gb* gb, const AggArgs& a, size_t smem, int
 
 static int32_t launch_fast(const qdb_gb* gb, const AggArgs& a, int32_t ptype, size_t smem, cudaStream_t st) {
     const ValKind vk = val_kind(gb->val_type);
+    if (a.kmod) {
+        if (gb->n_key_cols == 1 && gb->key_type == QDB_INT32) return launch_fast_i32_mod(a, vk, ptype, smem, st);
+        if (gb->n_key_cols == 1 && gb->key_type == QDB_INT64) return launch_fast_i64_mod(a, vk, ptype, smem, st);
+        return fail(QDB_ERR_INVALID, "gb_fast_kernel: key % m needs a single INT32 or INT64 key");
+    }
     if (gb->n_key_cols == 2) return launch_fast_comp(a, vk, ptype, smem, st);
     switch (gb->key_type) {
         case QDB_INT32: return launch_fast_i32(a, vk, ptype, smem, st);
@@ -614,12 +619,13 @@ int32_t qdb_gb_reset(qdb_gb* gb, void* stream) {
     return QDB_OK;
 }
 
-// A compressed-key call (kz) that the fast pass cannot take: the caller decompresses the keys instead.
+// A compressed-key call (kz) or a fused key % m call (km) that the fast pass cannot take: the caller decompresses the
+// keys, or materialises the remainder column, instead.
 constexpr int32_t kNotFused = -1;
 
 static int32_t process_impl(qdb_gb* gb, const void* const* key_cols, const uint64_t* const* key_nulls, const void* vals,
                             const uint64_t* val_nulls, int64_t n, const qdb_pred* pred, const int8_t* mask,
-                            void* stream, const AaflView* kz) {
+                            void* stream, const AaflView* kz, const ModMagic* km = nullptr) {
     if (!gb) return fail(QDB_ERR_INVALID, "qdb_gb_process: null table");
     if (n < 0) return fail(QDB_ERR_INVALID, "qdb_gb_process: negative row count");
     if (n == 0) return QDB_OK;
@@ -657,6 +663,13 @@ static int32_t process_impl(qdb_gb* gb, const void* const* key_cols, const uint6
         a.kz_off = kz->off;
         a.kz_len = kz->words_len;
     }
+    if (km) {
+        a.kmod = 1;
+        a.km_d = km->d;
+        a.km_m = km->m;
+        a.km_s1 = km->s1;
+        a.km_s2 = km->s2;
+    }
     a.knull0 = kn0;
     a.knull1 = kn1;
     a.vals = gb->val_type ? vals : nullptr;
@@ -685,7 +698,7 @@ static int32_t process_impl(qdb_gb* gb, const void* const* key_cols, const uint6
         const int32_t rc = process_fast(gb, a, pred, ptype, s, &used);
         if (rc != QDB_OK || used) return rc;
     }
-    if (kz) return kNotFused;
+    if (kz || km) return kNotFused;
 
     // Tile and stage plan: stages of about 32 KB (a stage costs a fixed hand-off between the producer and
     // the consumers, so small stages cannot reach the HBM bandwidth), three of them in the ring.
@@ -868,6 +881,30 @@ int32_t qdb_gb_process_aafl(qdb_gb* gb, const qdb_aafl_col* keys, const void* va
         dev_free(col, s);
     }
     dev_free(v.scratch, s);  // stream-ordered: after the pass that reads it
+    return rc;
+}
+
+int32_t qdb_gb_process_mod(qdb_gb* gb, const void* keys, int64_t key_mod, const void* vals, const qdb_pred* pred,
+                           int64_t n, void* stream) {
+    if (!gb || (n > 0 && !keys)) return fail(QDB_ERR_INVALID, "qdb_gb_process_mod: null argument");
+    if (gb->n_key_cols != 1 || (gb->key_type != QDB_INT32 && gb->key_type != QDB_INT64))
+        return fail(QDB_ERR_INVALID, "qdb_gb_process_mod: the table must have a single INT32 or INT64 key");
+    if (key_mod == 0) return fail(QDB_DIVISION_BY_ZERO, "qdb_gb_process_mod: modulo by zero");
+    if (key_mod == INT64_MIN || (gb->key_type == QDB_INT32 && (key_mod > INT32_MAX || key_mod < INT32_MIN)))
+        return fail(QDB_ERR_INVALID, "qdb_gb_process_mod: modulus out of the key type's range");
+    if (n == 0) return QDB_OK;
+    const ModMagic mm = mod_magic(static_cast<uint64_t>(key_mod < 0 ? -key_mod : key_mod));
+    const void* kc[1] = {keys};
+    int32_t rc = process_impl(gb, kc, nullptr, vals, nullptr, n, pred, nullptr, stream, nullptr, &mm);
+    if (rc != kNotFused) return rc;
+    // the fast pass does not apply: the remainder column first, as the dispatcher computes it
+    cudaStream_t s = as_stream(stream);
+    void* col = nullptr;
+    rc = dev_alloc(&col, static_cast<size_t>(n) * type_size(gb->key_type), s);
+    if (rc == QDB_OK) rc = qdb_arith_mod(gb->key_type, keys, key_mod, col, n, stream);
+    const void* mc[1] = {col};
+    if (rc == QDB_OK) rc = process_impl(gb, mc, nullptr, vals, nullptr, n, pred, nullptr, stream, nullptr);
+    dev_free(col, s);
     return rc;
 }
 

@@ -120,6 +120,11 @@ struct AggArgs {
     const uint8_t* kz_bits = nullptr;
     uint64_t kz_off = 0;
     int64_t kz_len = 0;
+    // Fused key % m (fast pass, a single integer key): each key is replaced by its C++ remainder by the modulus whose
+    // multiply-high constants these are (mod_signed) as it is read, before it is hashed.
+    int32_t kmod = 0;
+    int32_t km_s1 = 0, km_s2 = 0;
+    uint64_t km_d = 1, km_m = 1;
 };
 
 template <typename A, typename B>

@@ -299,6 +299,7 @@ constexpr int FM_SUM = 1;
 constexpr int FM_MM = 2;
 constexpr int FM_VALS = 4;
 constexpr int FM_KZ = 8;  // the key column is an AAFL-compressed block (single key, not DOUBLE)
+constexpr int FM_KMOD = 16;  // keys are replaced by key % m as they are read (single INT32 or INT64 key)
 
 template <typename VT, int MODE>
 struct FastWarp {
@@ -639,6 +640,12 @@ __device__ __forceinline__ KT kz_ring(const unsigned char* keys, const uint8_t* 
 // ---------------------------------------------------------------------------------------------
 constexpr int kListCap = 192;  // list entries per warp: fewer than 64 carried plus a tile's 128
 
+// A key's C++ remainder by the call's modulus (the fused key % m variant).
+template <typename KT>
+__device__ __forceinline__ KT kmod_key(const AggArgs& a, KT k) {
+    return static_cast<KT>(mod_signed(static_cast<int64_t>(k), a.km_d, a.km_m, a.km_s1, a.km_s2));
+}
+
 template <typename KT, bool COMP, typename VT, typename PT, int MODE>
 __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
@@ -648,6 +655,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
     constexpr bool VFLOAT = std::is_floating_point<VT>::value;
     constexpr bool VALS = (MODE & FM_VALS) != 0;
     constexpr bool KZ = !COMP && (MODE & FM_KZ) != 0;
+    constexpr bool KMOD = !COMP && !KZ && (MODE & FM_KMOD) != 0 && std::is_integral<KT>::value;
     using PL = typename std::conditional<HAS_PRED, PT, int32_t>::type;
     constexpr int PW = sizeof(PL);
 
@@ -870,6 +878,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
                         const int i = HAS_PRED ? list[act[u] ? e : e0] : w0 + (act[u] ? e : e0);
                         if constexpr (COMP) kw[u] = composite_word(static_cast<int32_t>(k0p[i]), static_cast<int32_t>(k1p[i]));
                         else if constexpr (KZ) kw[u] = key_word(kz_key<KT>(a, base + i));
+                        else if constexpr (KMOD) kw[u] = key_word(kmod_key<KT>(a, k0p[i]));
                         else kw[u] = key_word(k0p[i]);
                         if constexpr (VALS) v[u] = vp[i];
                         else v[u] = VT{};
@@ -884,6 +893,20 @@ __global__ void __launch_bounds__(kFastThreads, 1) gb_fast_kernel(const AggArgs 
             // The next tile of this CTA is staged too: rows left over may wait for it.
             const bool keep_going = carry && !full && q + 1 < my_tiles && tile + gridDim.x < a.full_tiles;
             const int g0 = s * kFastT + warp * kFastR;  // ring index of the warp's first row in this stage
+            if constexpr (KMOD) {
+                if (!full) {
+                    // Fused key % m: the warp replaces its own rows' keys in the stage by their remainders (no other
+                    // warp reads them), then fences its writes against the producer's next copy into the stage.
+                    KT* wk = const_cast<KT*>(rk0);
+#pragma unroll
+                    for (int j = 0; j < kFastSeg; ++j) {
+                        const int g = g0 + 32 * j + lane;
+                        wk[g] = static_cast<KT>(mod_signed(static_cast<int64_t>(wk[g]), a.km_d, a.km_m, a.km_s1, a.km_s2));
+                    }
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                }
+            }
             int total = lc;
             if (!full) {
                 if constexpr (HAS_PRED) {
@@ -1150,46 +1173,51 @@ inline int fast_mode(const AggArgs& a) {
     return (mm | sum) ? (FM_VALS | mm | sum) : 0;
 }
 
-// The compressed-key variant exists for single keys other than DOUBLE; plain keys run the kernel without it.
-template <typename KT, bool COMP, typename VT, typename PT, int MODE>
+// The compressed-key variant exists for single keys other than DOUBLE; plain keys run the kernel without it.  KM
+// selects the fused key % m variant (instantiated in its own translation units, fast_i32_mod.cu and fast_i64_mod.cu).
+template <typename KT, bool COMP, typename VT, typename PT, int MODE, bool KM>
 int32_t launch_fast_z(const AggArgs& a, size_t smem, cudaStream_t st) {
-    if constexpr (!COMP && !std::is_same<KT, double>::value) {
-        if (a.kz) return launch_fast_t<KT, COMP, VT, PT, MODE | FM_KZ>(a, smem, st);
+    if constexpr (KM) {
+        return launch_fast_t<KT, COMP, VT, PT, MODE | FM_KMOD>(a, smem, st);
+    } else {
+        if constexpr (!COMP && !std::is_same<KT, double>::value) {
+            if (a.kz) return launch_fast_t<KT, COMP, VT, PT, MODE | FM_KZ>(a, smem, st);
+        }
+        if (a.kz) return fail(QDB_ERR_INVALID, "gb_fast_kernel: compressed keys need a single INT32, INT64 or FLOAT key");
+        return launch_fast_t<KT, COMP, VT, PT, MODE>(a, smem, st);
     }
-    if (a.kz) return fail(QDB_ERR_INVALID, "gb_fast_kernel: compressed keys need a single INT32, INT64 or FLOAT key");
-    return launch_fast_t<KT, COMP, VT, PT, MODE>(a, smem, st);
 }
 
-template <typename KT, bool COMP, typename VT, typename PT>
+template <typename KT, bool COMP, typename VT, typename PT, bool KM>
 int32_t launch_fast_m(const AggArgs& a, size_t smem, cudaStream_t st) {
     switch (fast_mode(a)) {
-        case FM_VALS | FM_SUM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM>(a, smem, st);
-        case FM_VALS | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_MM>(a, smem, st);
-        case FM_VALS | FM_SUM | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM | FM_MM>(a, smem, st);
+        case FM_VALS | FM_SUM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM, KM>(a, smem, st);
+        case FM_VALS | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_MM, KM>(a, smem, st);
+        case FM_VALS | FM_SUM | FM_MM: return launch_fast_z<KT, COMP, VT, PT, FM_VALS | FM_SUM | FM_MM, KM>(a, smem, st);
         default: return fail(QDB_ERR_INVALID, "gb_fast_kernel: unsupported aggregate set");
     }
 }
 
-template <typename KT, bool COMP, typename PT>
+template <typename KT, bool COMP, typename PT, bool KM>
 int32_t launch_fast_v(const AggArgs& a, ValKind vk, size_t smem, cudaStream_t st) {
-    if (fast_mode(a) == 0) return launch_fast_z<KT, COMP, int32_t, PT, 0>(a, smem, st);
+    if (fast_mode(a) == 0) return launch_fast_z<KT, COMP, int32_t, PT, 0, KM>(a, smem, st);
     switch (vk) {
-        case VK_I32: return launch_fast_m<KT, COMP, int32_t, PT>(a, smem, st);
-        case VK_I64: return launch_fast_m<KT, COMP, int64_t, PT>(a, smem, st);
-        case VK_F32: return launch_fast_m<KT, COMP, float, PT>(a, smem, st);
-        case VK_F64: return launch_fast_m<KT, COMP, double, PT>(a, smem, st);
+        case VK_I32: return launch_fast_m<KT, COMP, int32_t, PT, KM>(a, smem, st);
+        case VK_I64: return launch_fast_m<KT, COMP, int64_t, PT, KM>(a, smem, st);
+        case VK_F32: return launch_fast_m<KT, COMP, float, PT, KM>(a, smem, st);
+        case VK_F64: return launch_fast_m<KT, COMP, double, PT, KM>(a, smem, st);
         default: return fail(QDB_ERR_INVALID, "unsupported value type");
     }
 }
 
-template <typename KT, bool COMP>
+template <typename KT, bool COMP, bool KM = false>
 int32_t launch_fast_k(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st) {
     switch (ptype) {
-        case 0: return launch_fast_v<KT, COMP, NoPred>(a, vk, smem, st);
-        case QDB_INT32: return launch_fast_v<KT, COMP, int32_t>(a, vk, smem, st);
-        case QDB_INT64: return launch_fast_v<KT, COMP, int64_t>(a, vk, smem, st);
-        case QDB_FLOAT: return launch_fast_v<KT, COMP, float>(a, vk, smem, st);
-        case QDB_DOUBLE: return launch_fast_v<KT, COMP, double>(a, vk, smem, st);
+        case 0: return launch_fast_v<KT, COMP, NoPred, KM>(a, vk, smem, st);
+        case QDB_INT32: return launch_fast_v<KT, COMP, int32_t, KM>(a, vk, smem, st);
+        case QDB_INT64: return launch_fast_v<KT, COMP, int64_t, KM>(a, vk, smem, st);
+        case QDB_FLOAT: return launch_fast_v<KT, COMP, float, KM>(a, vk, smem, st);
+        case QDB_DOUBLE: return launch_fast_v<KT, COMP, double, KM>(a, vk, smem, st);
         default: return fail(QDB_ERR_INVALID, "unsupported predicate column type");
     }
 }
@@ -1207,6 +1235,8 @@ int32_t launch_fspill_m(const AggArgs& a, size_t smem, int64_t grid, int32_t sli
 // Per-key-type entry points of the fast pass, each instantiated in its key type's translation unit.
 int32_t launch_fast_i32(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
 int32_t launch_fast_i64(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
+int32_t launch_fast_i32_mod(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
+int32_t launch_fast_i64_mod(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
 int32_t launch_fast_f32(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
 int32_t launch_fast_f64(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);
 int32_t launch_fast_comp(const AggArgs& a, ValKind vk, int32_t ptype, size_t smem, cudaStream_t st);

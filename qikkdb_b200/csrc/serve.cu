@@ -21,7 +21,6 @@
 
 namespace qdb {
 
-int32_t arith_mod_narrow(const int64_t* in, int64_t modulus, int32_t* out, int64_t n, cudaStream_t s);
 
 static int64_t now_ns() {
     return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now().time_since_epoch())
@@ -60,9 +59,6 @@ struct Slot {
     // a query routed through the single-query operators (one per slot): its table and key % m column
     bool plain = false;
     qdb_gb* gb = nullptr;
-    int32_t gb_key_type = 0;      // the table's key type: INT32 for an int64 key % m narrowed to int32
-    void* modcol = nullptr;       // kept across queries, grown on demand
-    int64_t modcol_bytes = 0;
 };
 
 // Sample of a key column (strided rows) kept per column for the cardinality estimates.
@@ -245,8 +241,8 @@ static void release_plain(Slot& sl) {
     sl.plain = false;
 }
 
-// Launches one query on a free slot through the single-query operators, as the dispatcher runs it: the key % m
-// column (GPUBinary modulo), a table of the query's capacity, ProcessBlock with the fused WHERE, completion event.
+// Launches one query on a free slot through the single-query operators: a table of the query's capacity, ProcessBlock
+// of key % m (the dispatcher's GPUBinary modulo column fused into the pass) with the fused WHERE, completion event.
 static void launch_plain(qdb_server* sv, Slot& sl, uint64_t id) {
     Ticket* tk;
     {
@@ -260,35 +256,16 @@ static void launch_plain(qdb_server* sv, Slot& sl, uint64_t id) {
     sl.busy = true;
     sl.plain = true;
     const qdb_gb_query& q = tk->q;
-    const void* key = q.keys;
-    int32_t rc = QDB_OK;
-    // an int64 key % m with m <= INT32_MAX groups by an int32 column of the same values
-    const bool narrow = q.key_type == QDB_INT64 && q.key_mod > 0 && q.key_mod <= INT32_MAX;
-    sl.gb_key_type = narrow ? QDB_INT32 : q.key_type;
-    if (q.key_mod > 0 && q.n_rows > 0) {
-        const int64_t bytes = q.n_rows * type_size(sl.gb_key_type);
-        if (bytes > sl.modcol_bytes) {
-            qdb_free(sl.modcol, sl.s);
-            sl.modcol = nullptr;
-            sl.modcol_bytes = 0;
-            rc = qdb_malloc(&sl.modcol, bytes, sl.s);
-            if (rc == QDB_OK) sl.modcol_bytes = bytes;
-        }
-        if (rc == QDB_OK) {
-            if (narrow)
-                rc = arith_mod_narrow(static_cast<const int64_t*>(q.keys), q.key_mod, static_cast<int32_t*>(sl.modcol),
-                                      q.n_rows, sl.s);
-            else
-                rc = qdb_arith_mod(q.key_type, q.keys, q.key_mod, sl.modcol, q.n_rows, sl.s);
-        }
-        key = sl.modcol;
-    }
-    if (rc == QDB_OK)
-        rc = qdb_gb_create(&sl.gb, q.agg_mask, sl.gb_key_type, 1, q.val_type, q.max_groups, QDB_PLACE_AUTO, sl.s);
+    int32_t rc = qdb_gb_create(&sl.gb, q.agg_mask, q.key_type, 1, q.val_type, q.max_groups, QDB_PLACE_AUTO, sl.s);
     if (rc == QDB_OK && q.n_rows > 0) {
-        const void* kc[1] = {key};
-        rc = qdb_gb_process(sl.gb, kc, nullptr, q.val_type ? q.vals : nullptr, nullptr, q.n_rows,
-                            q.pred.col ? &q.pred : nullptr, nullptr, sl.s);
+        const void* vals = q.val_type ? q.vals : nullptr;
+        const qdb_pred* pred = q.pred.col ? &q.pred : nullptr;
+        if (q.key_mod > 0) {
+            rc = qdb_gb_process_mod(sl.gb, q.keys, q.key_mod, vals, pred, q.n_rows, sl.s);
+        } else {
+            const void* kc[1] = {q.keys};
+            rc = qdb_gb_process(sl.gb, kc, nullptr, vals, nullptr, q.n_rows, pred, nullptr, sl.s);
+        }
     }
     if (rc == QDB_OK && cudaEventRecord(sl.ev, sl.s) != cudaSuccess) rc = QDB_ERR_CUDA;
     if (rc != QDB_OK) {
@@ -308,7 +285,7 @@ static int32_t read_plain_results(Slot& sl, Ticket* t) {
     void* ovals[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     int64_t g = 0;
     int32_t rc = qdb_gb_results_multi(sl.gb, na, aggs, okeys, nullptr, ovals, nullptr, &g, sl.s);
-    const int ks = type_size(sl.gb_key_type);
+    const int ks = type_size(q.key_type);
     const int vs = q.val_type ? type_size(q.val_type) : 8;
     // raw columns to the slot's pinned buffer (g <= max_groups, so they fit the result budget the query was admitted
     // against: at most 8 bytes per word of max_groups + 2 rows)
@@ -587,7 +564,6 @@ int32_t qdb_server_destroy(qdb_server* sv) {
         if (sl.s) cudaStreamSynchronize(sl.s);
         qdb_gb_batch_destroy(sl.b);
         if (sl.gb) qdb_gb_destroy(sl.gb);
-        qdb_free(sl.modcol, sl.s);
         if (sl.ev) cudaEventDestroy(sl.ev);
         if (sl.s) cudaStreamDestroy(sl.s);
         if (sl.h_counts) cudaFreeHost(sl.h_counts);

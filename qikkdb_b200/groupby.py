@@ -683,6 +683,16 @@ def process_aafl(table: "GroupByTable", keys: AaflBlock, values=None, pred=None,
         table.check(stream)
 
 
+def process_mod(table: "GroupByTable", keys, key_mod: int, values=None, pred=None, n: int | None = None,
+                stream=None, sync: bool = True):
+    """qdb_gb_process_mod: ProcessBlock of key % key_mod (the GPUBinary modulo column and the GROUP BY fused)."""
+    rows = int(keys.numel()) if n is None else int(n)
+    capi.check(capi.lib().qdb_gb_process_mod(table.handle, _ptr(keys), int(key_mod), _ptr(values),
+                                             C.byref(pred) if pred is not None else None, rows, _stream(stream)))
+    if sync:
+        table.check(stream)
+
+
 class ScalarAggregate:
     """Scalar aggregation over a query's blocks (qdb_scalar_*): COUNT, SUM, MIN, MAX (and AVG) of one value column,
     filtered by an optional `col OP constant` predicate and mask, NULL values skipped."""
