@@ -195,3 +195,21 @@ def test_server_plain_route_retries_when_table_overflows(columns):
     check(r, ref, q.aggs, False)
     assert srv.stats()["plain_queries"] == 1 + r["retries"]
     srv.close()
+
+
+def test_server_plain_route_without_modulus(columns):
+    """A query grouping by the key column itself (key_mod 0) on the single-query route: ProcessBlock over the column
+    as it is, its table sized by the server's estimate of the key's distinct count."""
+    h, d = columns
+    n = 1 << 16
+    keys = (h["k32"][:n] % 3000).astype(np.int64)
+    kd = torch.from_numpy(keys).cuda()
+    q = Query(kd, d["v32"][:n], ["min", "max", "sum", "count"], 0,
+              pred=(d["p"][:n], FilterConditions.less, 0.5, np.float32))
+    ref = oracle.groupby(keys, h["v32"][:n], pred=(h["p"][:n], FilterConditions.less, 0.5, np.float32, None))
+    srv = Server(max_batch=4, in_flight=2, table_budget=1 << 28, result_budget=1 << 26, plain_rows=1)
+    r = srv.wait(srv.submit(q))
+    assert r["status"] == 0 and r["batch_size"] == 1
+    check(r, ref, q.aggs, False)
+    assert srv.stats()["plain_queries"] >= 1
+    srv.close()
