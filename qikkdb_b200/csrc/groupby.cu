@@ -408,9 +408,13 @@ static int32_t process_fast(qdb_gb* gb, AggArgs a, const qdb_pred* pred, int32_t
         NB2 = static_cast<int>(budget2 / bucket_bytes);
         if (NB2 >= 64 && env_int("QDB_AGG_NO_SPILL", 0) == 0) {
             const uint64_t per = static_cast<uint64_t>(NB2);  // distinct keys per partition at half load
-            // At least four partitions per SM, so the spill pass's items balance over the SMs (the last wave of a
-            // pass with 1.7 items per SM leaves a quarter of them idle) ...
-            const uint64_t min_parts = next_pow2(4 * static_cast<uint64_t>(di.sm_count));
+            // At least two partitions per SM (512 on 148 SMs), so the spill pass's items balance over the SMs (the
+            // last wave of a pass with 1.7 items per SM leaves a quarter of them idle); more partitions measured
+            // slower (2^28-row filtered workload, aggregation + spill: 2.27 / 2.31 / 2.58 / 3.02 ms at 2 / 4 / 8 / 16
+            // per SM, and 2.32 ms at one) ...
+            const uint64_t min_parts =
+                next_pow2(static_cast<uint64_t>(std::max<int64_t>(1, env_int("QDB_SPILL_PARTS_PER_SM", 2))) *
+                          static_cast<uint64_t>(di.sm_count));
             const uint64_t parts = std::max(min_parts, next_pow2((static_cast<uint64_t>(gb->capacity) + per - 1) / per));
             int bits = 0;
             while ((1ull << bits) < parts) ++bits;
